@@ -1,0 +1,122 @@
+"""ctypes binding of ``libfpe_engine.so`` (the C ABI in include/fpe_engine.h).
+
+The library is built in-tree by :func:`fpe_option_b200.build.build_library`.
+There is no CPU fallback: loading fails loudly when the shared object is
+missing, and every compute entry point reports failure without a GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfpe_engine.so")
+
+d, i32, i64, vp = C.c_double, C.c_int32, C.c_int64, C.c_void_p
+dp = C.POINTER(C.c_double)
+ip = C.POINTER(C.c_int32)
+
+
+class FpeVecResult(C.Structure):
+    _fields_ = [("data", dp), ("len", i32)]
+
+
+class FpeVec2Result(C.Structure):
+    _fields_ = [("s_data", dp), ("s_len", i32), ("v_data", dp), ("v_len", i32)]
+
+
+class FpeGridPtsResult(C.Structure):
+    _fields_ = [("s_data", dp), ("s_len", i32), ("v_data", dp), ("v_len", i32),
+                ("sw_data", dp), ("vw_data", dp)]
+
+
+class FpeMatResult(C.Structure):
+    _fields_ = [("data", dp), ("n_rows", i32), ("n_cols", i32)]
+
+
+class FpeGreeksResult(C.Structure):
+    _fields_ = [("delta", dp), ("gamma", dp), ("vega", dp), ("len", i32)]
+
+
+class FpeOneshotResult(C.Structure):
+    _fields_ = [("price", dp), ("delta", dp), ("gamma", dp), ("vega", dp), ("len", i32)]
+
+
+class FpeContract(C.Structure):
+    _fields_ = [("kappa", d), ("theta", d), ("sigma", d), ("rho", d), ("r", d), ("T", d),
+                ("S0", d), ("V0", d), ("barrier", d), ("s_min", d), ("s_max", d),
+                ("n_s", i32), ("n_v", i32), ("option_type", i32), ("n_strikes", i32),
+                ("strikes", dp)]
+
+
+class FpeBatchOptions(C.Structure):
+    _fields_ = [("disc", i32), ("precision", i32), ("num_insert", i32), ("refine", i32),
+                ("rtol", d), ("atol", d), ("ic_sigma_s", d), ("ic_sigma_v", d), ("ic_sub", i32),
+                ("greeks", i32), ("rel_s", d), ("rel_v", d)]
+
+
+# Every symbol declared in include/fpe_engine.h.
+EXPORTED = [
+    "fpe_compute_create", "fpe_compute_destroy", "fpe_compute_knots", "fpe_compute_grid_points",
+    "fpe_compute_initial_condition", "fpe_compute_solve", "fpe_compute_pdf", "fpe_compute_price",
+    "fpe_compute_greeks", "fpe_price_oneshot", "fpe_compute_free_vec", "fpe_compute_free_vec2",
+    "fpe_compute_free_grid_pts", "fpe_compute_free_mat", "fpe_compute_free_greeks",
+    "fpe_compute_free_oneshot", "fpe_plan_create", "fpe_plan_run", "fpe_plan_results",
+    "fpe_plan_stats", "fpe_plan_sizes", "fpe_plan_destroy", "fpe_price_batch",
+    "fpe_compute_create_ex", "fpe_compute_basis_csr", "fpe_device_available",
+]
+
+_lib = None
+
+
+def load():
+    """Load the library (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"libfpe_engine.so not built ({LIB_PATH}); run fpe_option_b200.build.build_library()")
+    L = C.CDLL(LIB_PATH)
+    cp = vp
+    L.fpe_compute_create.restype = cp
+    L.fpe_compute_create.argtypes = [d] * 8 + [i32, i32, d, i32, i32, d, d]
+    L.fpe_compute_create_ex.restype = cp
+    L.fpe_compute_create_ex.argtypes = [d] * 8 + [i32, i32, d, i32, d, d,
+                                                  C.POINTER(FpeBatchOptions)]
+    L.fpe_compute_destroy.argtypes = [cp]
+    L.fpe_compute_knots.argtypes = [cp, C.POINTER(FpeVec2Result)]
+    L.fpe_compute_grid_points.argtypes = [cp, C.POINTER(FpeGridPtsResult)]
+    L.fpe_compute_initial_condition.argtypes = [cp, C.POINTER(FpeVecResult)]
+    L.fpe_compute_solve.argtypes = [cp, C.POINTER(FpeMatResult)]
+    L.fpe_compute_pdf.argtypes = [cp, C.POINTER(FpeMatResult)]
+    L.fpe_compute_price.argtypes = [cp, dp, i32, C.POINTER(FpeVecResult)]
+    L.fpe_compute_greeks.argtypes = [cp, dp, i32, d, d, C.POINTER(FpeGreeksResult)]
+    L.fpe_price_oneshot.argtypes = [d] * 8 + [dp, i32, d, i32, i32, i32, i32, d, d,
+                                              C.POINTER(FpeOneshotResult)]
+    L.fpe_compute_free_vec.argtypes = [C.POINTER(FpeVecResult)]
+    L.fpe_compute_free_vec2.argtypes = [C.POINTER(FpeVec2Result)]
+    L.fpe_compute_free_grid_pts.argtypes = [C.POINTER(FpeGridPtsResult)]
+    L.fpe_compute_free_mat.argtypes = [C.POINTER(FpeMatResult)]
+    L.fpe_compute_free_greeks.argtypes = [C.POINTER(FpeGreeksResult)]
+    L.fpe_compute_free_oneshot.argtypes = [C.POINTER(FpeOneshotResult)]
+    L.fpe_plan_create.restype = cp
+    L.fpe_plan_create.argtypes = [C.POINTER(FpeContract), i32, C.POINTER(FpeBatchOptions)]
+    L.fpe_plan_run.restype = i32
+    L.fpe_plan_run.argtypes = [cp, vp]
+    L.fpe_plan_results.restype = i32
+    L.fpe_plan_results.argtypes = [cp, dp, dp, dp, dp, ip]
+    L.fpe_plan_stats.restype = i32
+    L.fpe_plan_stats.argtypes = [cp, C.POINTER(C.c_int64)]
+    L.fpe_plan_sizes.restype = i32
+    L.fpe_plan_sizes.argtypes = [cp, ip, ip]
+    L.fpe_plan_destroy.argtypes = [cp]
+    L.fpe_price_batch.restype = i32
+    L.fpe_price_batch.argtypes = [C.POINTER(FpeContract), i32, C.POINTER(FpeBatchOptions),
+                                  dp, dp, dp, dp, ip]
+    L.fpe_compute_basis_csr.restype = i64
+    L.fpe_compute_basis_csr.argtypes = [cp, i32, ip, ip, ip, ip, dp]
+    L.fpe_device_available.restype = i32
+    L.fpe_device_available.argtypes = []
+    _lib = L
+    return L

@@ -1,0 +1,163 @@
+// Shared host/device layout of one batched Fokker-Planck solve.
+//
+// A batch is a list of independent solves.  Each solve owns one slot in three
+// arenas (FP64 data, int32 data, stage-system factors) whose offsets the host
+// computes from per-solve capacity bounds.  All kernels run one CTA per solve.
+#pragma once
+#include <stdint.h>
+
+#define FPE_BLOCK 256
+#define FPE_MAX_STRIKES 1024
+#define FPE_MAX_NDOF_V 64      // block size of the block-banded stage LU
+#define FPE_MAX_NDOF_S 160
+#define FPE_GMRES_M 10
+
+// Status word per solve (0 = ok).
+enum FpeStatus : int32_t {
+  FPE_OK = 0,
+  FPE_ERR_CAPACITY = 1,      // a discretization array exceeded its bound
+  FPE_ERR_UNSUPPORTED = 2,   // n_dof_v above the block-LU limit
+  FPE_ERR_SINGULAR = 3,      // zero pivot in a diagonal block
+  FPE_ERR_MAX_STEPS = 4,     // radau.mojo:257-263
+  FPE_ERR_STEP_UNDERFLOW = 5,// radau.mojo:274-281, :458-464
+  FPE_ERR_NONFINITE = 6,
+};
+
+// Per-solve counters written by the kernels (int32 arena, FPE_INFO_* slots).
+enum FpeInfo {
+  FPE_INFO_STATUS = 0,
+  FPE_INFO_NKNOT_S, FPE_INFO_NKNOT_V, FPE_INFO_NGRID_S, FPE_INFO_NGRID_V,
+  FPE_INFO_NQ_S, FPE_INFO_NQ_V, FPE_INFO_NDOF_S, FPE_INFO_NDOF_V,
+  FPE_INFO_ACCEPTED, FPE_INFO_REJECTED, FPE_INFO_NEWTON, FPE_INFO_GMRES, FPE_INFO_LU,
+  FPE_INFO_ADMM, FPE_INFO_REFINE, FPE_INFO_NSAVED,
+  FPE_INFO_COUNT = 20
+};
+
+struct FpeSolveDesc {
+  // Heston parameters (already revised for the barrier domain)
+  double kappa, theta, sigma, rho, r, T, S0, V0;
+  double smin, smax, vmin, vmax;
+  double barrier;
+  double rtol, atol;
+  double ic_sigma_s, ic_sigma_v;
+  int32_t type;          // 0..9; knock-ins are split into two solves by the host
+  int32_t n_s, n_v;      // knot-count inputs
+  int32_t left_neu, right_neu;
+  int32_t disc;          // 0 reference, 1 config
+  int32_t num_insert;
+  int32_t ic_sub;
+  int32_t strike_off, n_strikes;
+  int32_t save_traj;     // keep every accepted step (stepwise API)
+  int32_t traj_cap;      // max saved states
+  // capacities
+  int32_t cap_knot_s, cap_knot_v, cap_grid_s, cap_grid_v, cap_q_s, cap_q_v;
+  int32_t cap_dof_s, cap_dof_v;
+  // arena offsets (elements)
+  int64_t off_d;         // double arena
+  int64_t off_i;         // int32 arena
+  int64_t off_f;         // factor arena (bytes)
+  int64_t off_traj;      // trajectory arena (doubles), -1 when not saved
+};
+
+// Offsets of the sub-arrays inside one solve's double slot.  Computed
+// identically on host and device from the descriptor capacities.
+struct FpeDLayout {
+  int64_t knot_s, knot_v, grid_s, grid_v;
+  int64_t qx_s, qw_s, qp_s, qx_v, qw_v, qp_v;      // nodes: normalized, weight, physical
+  int64_t B_s, dB_s, B_v, dB_v;                     // 4 values per node
+  int64_t fac_s, fac_v;                             // raw 1-D Galerkin factors
+  int64_t op_s, op_v, D_s, D_v, m_s, m_v;           // scaled operator factors
+  int64_t proj, q0, y, qT;                          // vectors of length N
+  int64_t work;                                     // Radau/GMRES/ADMM work area
+  int64_t total;
+};
+
+struct FpeILayout {
+  int64_t info, c0_s, c0_v, rng_s, rng_v, total;
+};
+
+// Number of raw 1-D factors per axis and their order.
+//   s: 0 Ns = Bs^T W Bs, 1 Ss = dBs^T W s Bs, 2 Tss = dBs^T W s^2 dBs
+//   v: 0 Nv, 1 V2 = Bv^T W v Bv, 2 V3 = Bv^T W v dBv, 3 V4 = dBv^T W Bv,
+//      4 V5 = dBv^T W v Bv, 5 V6 = dBv^T W v dBv
+#define FPE_NFAC_S 3
+#define FPE_NFAC_V 6
+// Scaled operator factors (band 7, D-scaled):
+//   s: 0 As, 1 Ss~, 2 Tss~, 3 Ss~^T        v: 0 Av, 1 B1, 2 B2, 3 B3, 4 B4
+#define FPE_NOP_S 4
+#define FPE_NOP_V 5
+#define FPE_WORK_VECS 80   // N-length FP64 work vectors per solve
+
+#ifdef __CUDACC__
+#define FPE_HD __host__ __device__ __forceinline__
+#else
+#define FPE_HD inline
+#endif
+
+FPE_HD FpeDLayout fpe_dlayout(const FpeSolveDesc& d) {
+  FpeDLayout L;
+  int64_t o = 0;
+  auto take = [&](int64_t n) {
+    int64_t r = o;
+    o += (n + 7) & ~int64_t(7);
+    return r;
+  };
+  int64_t N = int64_t(d.cap_dof_s) * d.cap_dof_v;
+  L.knot_s = take(d.cap_knot_s);
+  L.knot_v = take(d.cap_knot_v);
+  L.grid_s = take(d.cap_grid_s);
+  L.grid_v = take(d.cap_grid_v);
+  L.qx_s = take(d.cap_q_s);
+  L.qw_s = take(d.cap_q_s);
+  L.qp_s = take(d.cap_q_s);
+  L.qx_v = take(d.cap_q_v);
+  L.qw_v = take(d.cap_q_v);
+  L.qp_v = take(d.cap_q_v);
+  L.B_s = take(4 * int64_t(d.cap_q_s));
+  L.dB_s = take(4 * int64_t(d.cap_q_s));
+  L.B_v = take(4 * int64_t(d.cap_q_v));
+  L.dB_v = take(4 * int64_t(d.cap_q_v));
+  L.fac_s = take(int64_t(FPE_NFAC_S) * d.cap_dof_s * 7);
+  L.fac_v = take(int64_t(FPE_NFAC_V) * d.cap_dof_v * 7);
+  L.op_s = take(int64_t(FPE_NOP_S) * d.cap_dof_s * 7);
+  L.op_v = take(int64_t(FPE_NOP_V) * d.cap_dof_v * 7);
+  L.D_s = take(d.cap_dof_s);
+  L.D_v = take(d.cap_dof_v);
+  L.m_s = take(d.cap_dof_s);
+  L.m_v = take(d.cap_dof_v);
+  L.proj = take(N);
+  L.q0 = take(N);
+  L.y = take(N);
+  L.qT = take(N);
+  int64_t dense = int64_t(d.cap_dof_s) * d.cap_dof_s + int64_t(d.cap_dof_v) * d.cap_dof_v;
+  L.work = take(int64_t(FPE_WORK_VECS) * N + 4 * dense + 256);
+  L.total = o;
+  return L;
+}
+
+FPE_HD FpeILayout fpe_ilayout(const FpeSolveDesc& d) {
+  FpeILayout L;
+  int64_t o = 0;
+  auto take = [&](int64_t n) {
+    int64_t r = o;
+    o += (n + 3) & ~int64_t(3);
+    return r;
+  };
+  L.info = take(FPE_INFO_COUNT);
+  L.c0_s = take(d.cap_q_s);
+  L.c0_v = take(d.cap_q_v);
+  L.rng_s = take(2 * int64_t(d.cap_dof_s));
+  L.rng_v = take(2 * int64_t(d.cap_dof_v));
+  L.total = o;
+  return L;
+}
+
+// Bytes of stage-system factor storage: one real block-banded LU (ns block
+// rows x 7 blocks of nv x nv) of element size esz, plus the same for the
+// complex system when requested (2 * esz per entry).
+FPE_HD int64_t fpe_factor_bytes(const FpeSolveDesc& d, int esz, int with_complex) {
+  int64_t blocks = int64_t(d.cap_dof_s) * 7 * d.cap_dof_v * d.cap_dof_v;
+  int64_t b = blocks * esz;
+  if (with_complex) b += blocks * 2 * esz;
+  return (b + 255) & ~int64_t(255);
+}

@@ -1,0 +1,231 @@
+/** @file fpe_engine.h
+ *  @brief C ABI of the B200 Heston Fokker-Planck pricing engine.
+ *
+ *  Part 1 is a drop-in for the reference C ABI (elevenwang-creator/FPE_option,
+ *  cpp/include/fpe_engine.h): the same 16 symbols, argument order, struct
+ *  layouts (sizes pinned by static_assert), ownership and error behaviour.
+ *  Every result array is allocated by the library and released with the
+ *  matching fpe_compute_free_* call; failures return NULL data and zero length.
+ *
+ *  Part 2 adds the batched entry points: thousands of contracts with
+ *  different parameters, barriers and grid sizes priced in one launch
+ *  sequence on one GPU.  There is no CPU fallback: when no CUDA device is
+ *  usable every entry point fails (NULL handle / negative return code).
+ */
+#ifndef FPE_ENGINE_H
+#define FPE_ENGINE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================= Part 1: reference C ABI ======================== */
+
+/** Opaque handle to a stepwise pricing pipeline. */
+typedef struct FpeCompute FpeCompute;
+
+/** reference cpp/include/fpe_engine.h:21-24 */
+struct FpeVecResult {
+    double* data;
+    int32_t len;
+};
+
+/** reference cpp/include/fpe_engine.h:27-32 */
+struct FpeVec2Result {
+    double* s_data;
+    int32_t s_len;
+    double* v_data;
+    int32_t v_len;
+};
+
+/** reference cpp/include/fpe_engine.h:35-42 */
+struct FpeGridPtsResult {
+    double* s_data;
+    int32_t s_len;
+    double* v_data;
+    int32_t v_len;
+    double* sw_data;
+    double* vw_data;
+};
+
+/** reference cpp/include/fpe_engine.h:45-49 (row-major) */
+struct FpeMatResult {
+    double* data;
+    int32_t n_rows;
+    int32_t n_cols;
+};
+
+/** reference cpp/include/fpe_engine.h:52-57 */
+struct FpeGreeksResult {
+    double* delta;
+    double* gamma;
+    double* vega;
+    int32_t len;
+};
+
+/** reference cpp/include/fpe_engine.h:60-66 */
+struct FpeOneshotResult {
+    double* price;
+    double* delta;
+    double* gamma;
+    double* vega;
+    int32_t len;
+};
+
+/** Replaces reference fpe_compute_create (cpp/include/fpe_engine.h:87-94).
+ *  s_min < 0 -> 0; s_max <= 0 -> 3*S0; num_insert <= 0 -> 251.
+ *  Returns NULL on invalid parameters or when no GPU is usable. */
+extern FpeCompute* fpe_compute_create(
+    double kappa, double theta, double sigma, double rho,
+    double r, double T, double S0, double V0,
+    int32_t n_s, int32_t n_v,
+    double barrier, int32_t option_type,
+    int32_t num_insert,
+    double s_min, double s_max);
+
+/** Replaces reference fpe_compute_destroy (cpp/include/fpe_engine.h:97). */
+extern void fpe_compute_destroy(FpeCompute* ptr);
+
+/** Replaces reference fpe_compute_knots (cpp/include/fpe_engine.h:103). */
+extern void fpe_compute_knots(FpeCompute* ptr, struct FpeVec2Result* result);
+
+/** Replaces reference fpe_compute_grid_points (cpp/include/fpe_engine.h:109). */
+extern void fpe_compute_grid_points(FpeCompute* ptr, struct FpeGridPtsResult* result);
+
+/** Replaces reference fpe_compute_initial_condition (cpp/include/fpe_engine.h:115). */
+extern void fpe_compute_initial_condition(FpeCompute* ptr, struct FpeVecResult* result);
+
+/** Replaces reference fpe_compute_solve (cpp/include/fpe_engine.h:121):
+ *  every accepted step (t = 0 included) x degrees of freedom, row-major. */
+extern void fpe_compute_solve(FpeCompute* ptr, struct FpeMatResult* result);
+
+/** Replaces reference fpe_compute_pdf (cpp/include/fpe_engine.h:127). */
+extern void fpe_compute_pdf(FpeCompute* ptr, struct FpeMatResult* result);
+
+/** Replaces reference fpe_compute_price (cpp/include/fpe_engine.h:135-140). */
+extern void fpe_compute_price(FpeCompute* ptr, const double* K, int32_t n_K,
+                              struct FpeVecResult* result);
+
+/** Replaces reference fpe_compute_greeks (cpp/include/fpe_engine.h:150-157).
+ *  rel_s / rel_v == 0 -> 0.01 / 0.1. */
+extern void fpe_compute_greeks(FpeCompute* ptr, const double* K, int32_t n_K,
+                               double rel_s, double rel_v, struct FpeGreeksResult* result);
+
+/** Replaces reference fpe_price_oneshot (cpp/include/fpe_engine.h:164-173):
+ *  price + central finite-difference Greeks (5 solves, 10 for knock-ins),
+ *  all run as one batch. */
+extern void fpe_price_oneshot(
+    double kappa, double theta, double sigma, double rho,
+    double r, double T, double S0, double V0,
+    const double* K, int32_t n_K,
+    double barrier, int32_t option_type,
+    int32_t n_s, int32_t n_v,
+    int32_t num_insert,
+    double s_min, double s_max,
+    struct FpeOneshotResult* result);
+
+/** Replace reference fpe_compute_free_* (cpp/include/fpe_engine.h:176-186). */
+extern void fpe_compute_free_vec(struct FpeVecResult* r);
+extern void fpe_compute_free_vec2(struct FpeVec2Result* r);
+extern void fpe_compute_free_grid_pts(struct FpeGridPtsResult* r);
+extern void fpe_compute_free_mat(struct FpeMatResult* r);
+extern void fpe_compute_free_greeks(struct FpeGreeksResult* r);
+extern void fpe_compute_free_oneshot(struct FpeOneshotResult* r);
+
+/* ================== Part 2: batched pricing (additions) ================= */
+
+/** One contract.  option_type 0-9 as in the reference (down/up, in/out,
+ *  call/put, european).  Knock-ins are priced by in-out parity (two solves).
+ *  s_min < 0 -> 0; s_max <= 0 -> 3*S0. */
+typedef struct FpeContract {
+    double kappa, theta, sigma, rho, r, T, S0, V0;
+    double barrier, s_min, s_max;
+    int32_t n_s, n_v, option_type, n_strikes;
+    const double* strikes;  /* host pointer, n_strikes values */
+} FpeContract;
+
+/** Batch options (zero-initialised = reference Pricer defaults in FP64). */
+typedef struct FpeBatchOptions {
+    int32_t disc;        /* 0 reference discretization, 1 config discretization */
+    int32_t precision;   /* 0 FP64 stage factors, 1 FP32 factors + FP64 refinement */
+    int32_t num_insert;  /* reference discretization grid size (<= 0 -> 50) */
+    int32_t refine;      /* refinement sweeps in precision 1 (< 0 -> 2, 0 -> 2) */
+    double rtol, atol;   /* Radau tolerances (<= 0 -> 1e-4 / 1e-6) */
+    double ic_sigma_s, ic_sigma_v; /* config IC widths (<= 0 -> 0.6 / 0.004) */
+    int32_t ic_sub;      /* config IC quadrature subintervals per span (<= 0 -> 8) */
+    int32_t greeks;      /* 1: delta/gamma/vega by 4 bumped solves per contract */
+    double rel_s, rel_v; /* Greeks bumps relative to S0 / V0 (<= 0 -> 0.01 / 0.1) */
+} FpeBatchOptions;
+
+/** Status codes written per strike slot of a batch. */
+#define FPE_STATUS_OK 0
+#define FPE_STATUS_CAPACITY 1
+#define FPE_STATUS_UNSUPPORTED 2
+#define FPE_STATUS_SINGULAR 3
+#define FPE_STATUS_MAX_STEPS 4
+#define FPE_STATUS_STEP_UNDERFLOW 5
+#define FPE_STATUS_NONFINITE 6
+#define FPE_STATUS_INVALID 16
+
+/** A prepared batch: descriptors and strikes resident on the device.
+ *  No reference counterpart (the reference prices one contract per call). */
+typedef struct FpePlan FpePlan;
+
+/** Build a plan (host packing + one host-to-device copy). NULL on failure. */
+extern FpePlan* fpe_plan_create(const FpeContract* contracts, int32_t n,
+                                const FpeBatchOptions* opt);
+/** Enqueue the whole solve pipeline on a CUDA stream (NULL = the library's
+ *  stream); asynchronous.  Returns the number of kernel launches, < 0 on error. */
+extern int32_t fpe_plan_run(FpePlan* plan, void* cuda_stream);
+/** Wait for the plan, copy results to the host and combine parity / Greeks.
+ *  Arrays hold one value per strike in contract order (delta/gamma/vega may
+ *  be NULL; they are filled only when opt->greeks was set).  Returns 0 when
+ *  every solve succeeded, otherwise the first non-zero status. */
+extern int32_t fpe_plan_results(FpePlan* plan, double* prices, double* delta, double* gamma,
+                                double* vega, int32_t* status);
+/** Aggregated solver counters: out[0] solves, [1] accepted steps, [2] rejected,
+ *  [3] Newton iterations, [4] GMRES iterations, [5] LU factorizations,
+ *  [6] ADMM iterations, [7] max n_dof_s, [8] max n_dof_v, [9] total dofs. */
+extern int32_t fpe_plan_stats(FpePlan* plan, int64_t* out);
+/** Number of strike results and of device solves in the plan. */
+extern int32_t fpe_plan_sizes(FpePlan* plan, int32_t* n_results, int32_t* n_solves);
+extern void fpe_plan_destroy(FpePlan* plan);
+
+/** One-call batch: plan, run, results, destroy. */
+extern int32_t fpe_price_batch(const FpeContract* contracts, int32_t n,
+                               const FpeBatchOptions* opt, double* prices, double* delta,
+                               double* gamma, double* vega, int32_t* status);
+
+/** Stepwise pipeline with explicit options (the reference create uses Compute
+ *  defaults: reference discretization, rtol 1e-4, atol 1e-6). */
+extern FpeCompute* fpe_compute_create_ex(
+    double kappa, double theta, double sigma, double rho,
+    double r, double T, double S0, double V0,
+    int32_t n_s, int32_t n_v, double barrier, int32_t option_type,
+    double s_min, double s_max, const FpeBatchOptions* opt);
+
+/** Recombined 1-D basis of a pipeline as CSR (which: 0 Bs, 1 dBs, 2 Bv, 3 dBv);
+ *  returns nnz; arrays are filled when non-NULL. */
+extern int64_t fpe_compute_basis_csr(FpeCompute* ptr, int32_t which, int32_t* n_rows,
+                                     int32_t* n_cols, int32_t* indptr, int32_t* indices,
+                                     double* data);
+
+/** Device availability: 1 when a CUDA device can run the kernels. */
+extern int32_t fpe_device_available(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#ifdef __cplusplus
+static_assert(sizeof(struct FpeVecResult) == 16, "FpeVecResult layout mismatch");
+static_assert(sizeof(struct FpeVec2Result) == 32, "FpeVec2Result layout mismatch");
+static_assert(sizeof(struct FpeGridPtsResult) == 48, "FpeGridPtsResult layout mismatch");
+static_assert(sizeof(struct FpeMatResult) == 16, "FpeMatResult layout mismatch");
+static_assert(sizeof(struct FpeGreeksResult) == 32, "FpeGreeksResult layout mismatch");
+static_assert(sizeof(struct FpeOneshotResult) == 40, "FpeOneshotResult layout mismatch");
+#endif
+
+#endif

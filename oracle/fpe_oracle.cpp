@@ -435,6 +435,7 @@ struct Options {
   double ic_sigma_s = 0.6, ic_sigma_v = 0.004;
   bool nnls_exact = false;
   int ic_sub = 8;
+  bool complex_direct = false;
 };
 
 static Options options_from(const OrcOptions* o, int default_num_insert) {
@@ -449,6 +450,7 @@ static Options options_from(const OrcOptions* o, int default_num_insert) {
   if (o->ic_sigma_v > 0) r.ic_sigma_v = o->ic_sigma_v;
   r.nnls_exact = o->nnls_exact != 0;
   if (o->ic_sub > 0) r.ic_sub = o->ic_sub;
+  r.complex_direct = o->complex_direct != 0;
   return r;
 }
 
@@ -679,27 +681,28 @@ static Ops build_ops(const Factors& f) {
 // replacing SparseLU (sparse_lu.mojo:78-352): same pivot rule (first max |.|),
 // same drop tolerances (|u| < 1e-14, |l-numerator| <= 1e-14).
 // ---------------------------------------------------------------------------
-struct BandLU {
+template <class T>
+struct BandLUT {
   int n = 0, kl = 0, ku = 0, w = 0;
-  Vec a;  // row i holds columns [i-kl, i+kl+ku]
-  Vec L;  // n x kl multipliers
+  std::vector<T> a;  // row i holds columns [i-kl, i+kl+ku]
+  std::vector<T> L;  // n x kl multipliers
   std::vector<int> piv;
-  Vec diag;
-  double& at(int i, int j) { return a[size_t(i) * w + (j - i + kl)]; }
+  std::vector<T> diag;
+  T& at(int i, int j) { return a[size_t(i) * w + (j - i + kl)]; }
 
   void init(int nn, int kll, int kuu) {
     n = nn;
     kl = kll;
     ku = kuu;
     w = 2 * kl + ku + 1;
-    a.assign(size_t(n) * w, 0.0);
-    L.assign(size_t(n) * std::max(kl, 1), 0.0);
+    a.assign(size_t(n) * w, T(0.0));
+    L.assign(size_t(n) * std::max(kl, 1), T(0.0));
     piv.assign(n, 0);
-    diag.assign(n, 1.0);
+    diag.assign(n, T(1.0));
   }
   // A given as CSR with all entries inside [i-kl, i+ku].
   void factor(const CSR& A) {
-    std::fill(a.begin(), a.end(), 0.0);
+    std::fill(a.begin(), a.end(), T(0.0));
     for (int i = 0; i < n; ++i)
       for (int p = A.indptr[i]; p < A.indptr[i + 1]; ++p) at(i, A.indices[p]) = A.data[p];
     run();
@@ -708,59 +711,61 @@ struct BandLU {
     for (int k = 0; k < n; ++k) {
       int imax = std::min(k + kl, n - 1);
       int jmax = std::min(k + kl + ku, n - 1);
-      double pv = at(k, k);
+      T pv = at(k, k);
       int pr = k;
       for (int i = k + 1; i <= imax; ++i)
-        if (std::fabs(at(i, k)) > std::fabs(pv)) {
+        if (std::abs(at(i, k)) > std::abs(pv)) {
           pv = at(i, k);
           pr = i;
         }
       piv[k] = pr;
-      if (std::fabs(pv) < 1e-14) {  // sparse_lu.mojo:170-174 (column skipped)
-        for (int i = k; i <= imax; ++i) at(i, k) = 0.0;
-        for (int i = k + 1; i <= imax; ++i) L[size_t(k) * kl + (i - k - 1)] = 0.0;
+      if (std::abs(pv) < 1e-14) {  // sparse_lu.mojo:170-174 (column skipped)
+        for (int i = k; i <= imax; ++i) at(i, k) = T(0.0);
+        for (int i = k + 1; i <= imax; ++i) L[size_t(k) * kl + (i - k - 1)] = T(0.0);
         piv[k] = k;
-        diag[k] = 1.0;
+        diag[k] = T(1.0);
         continue;
       }
       if (pr != k)
         for (int j = k; j <= jmax; ++j) std::swap(at(k, j), at(pr, j));
       for (int j = k + 1; j <= jmax; ++j)
-        if (std::fabs(at(k, j)) < 1e-14) at(k, j) = 0.0;
+        if (std::abs(at(k, j)) < 1e-14) at(k, j) = T(0.0);
       diag[k] = at(k, k);
-      double inv = 1.0 / at(k, k);
+      T inv = T(1.0) / at(k, k);
       for (int i = k + 1; i <= imax; ++i) {
-        double wv = at(i, k);
-        double l = 0.0;
-        if (std::fabs(wv) > 1e-14) l = wv * inv;
+        T wv = at(i, k);
+        T l = T(0.0);
+        if (std::abs(wv) > 1e-14) l = wv * inv;
         L[size_t(k) * kl + (i - k - 1)] = l;
-        at(i, k) = 0.0;
-        if (l == 0.0) continue;
+        at(i, k) = T(0.0);
+        if (l == T(0.0)) continue;
         for (int j = k + 1; j <= jmax; ++j) {
-          double u = at(k, j);
-          if (u != 0.0) at(i, j) -= l * u;
+          T u = at(k, j);
+          if (u != T(0.0)) at(i, j) -= l * u;
         }
       }
     }
   }
-  void solve(double* b) const {
+  void solve(T* b) const {
     for (int k = 0; k < n; ++k) {
       int p = piv[k];
       if (p != k) std::swap(b[k], b[p]);
-      double bk = b[k];
-      if (bk == 0.0) continue;
+      T bk = b[k];
+      if (bk == T(0.0)) continue;
       int imax = std::min(k + kl, n - 1);
       for (int i = k + 1; i <= imax; ++i) b[i] -= L[size_t(k) * kl + (i - k - 1)] * bk;
     }
     for (int k = n - 1; k >= 0; --k) {
       int jmax = std::min(k + kl + ku, n - 1);
-      double s = b[k];
-      const double* row = &a[size_t(k) * w + kl];
+      T s = b[k];
+      const T* row = &a[size_t(k) * w + kl];
       for (int j = k + 1; j <= jmax; ++j) s -= row[j - k] * b[j];
       b[k] = s / diag[k];
     }
   }
 };
+using BandLU = BandLUT<double>;
+using CBandLU = BandLUT<std::complex<double>>;
 
 // ---------------------------------------------------------------------------
 // IC NNLS.  osqp.mojo:52-159 (ADMM) and an exact primal-dual active-set solve
@@ -967,6 +972,7 @@ static double pow_pos(double x, double p) { return x <= 0.0 ? 0.0 : std::pow(x, 
 struct RadauSolver {
   double rtol, atol, max_step, first_step;
   bool save_all = true;
+  bool complex_direct = false;  // exact complex stage solve instead of GMRES(10)
 
   // radau.mojo:882-1146 left-preconditioned GMRES on the real 2n form of
   // (ALPH + i BETA) M + h_lu K with P = diag(E1, E1).
@@ -1110,6 +1116,9 @@ struct RadauSolver {
     kl = std::max(kl, csr_kl(M));
     BandLU lu;
     lu.init(n, kl, kl);
+    CBandLU clu;
+    if (complex_direct) clu.init(n, kl, kl);
+    std::vector<std::complex<double>> cb(complex_direct ? n : 0);
     // E1 = U1 M + h K and E_diag = ALPH M + h K on the union pattern (M and K
     // share the 7x7 stencil here): radau.mojo:632-880.
     CSR E1 = M, Ed = M;
@@ -1144,6 +1153,13 @@ struct RadauSolver {
       if (need_lu) {
         update_sys(h);
         lu.factor(E1);
+        if (complex_direct) {
+          std::fill(clu.a.begin(), clu.a.end(), std::complex<double>(0.0));
+          for (int i = 0; i < n; ++i)
+            for (int p = M.indptr[i]; p < M.indptr[i + 1]; ++p)
+              clu.at(i, M.indices[p]) = std::complex<double>(Ed.data[p], BETA * M.data[p]);
+          clu.run();
+        }
         res.lu++;
         h_lu = h;
       }
@@ -1193,7 +1209,16 @@ struct RadauSolver {
         }
         dF1 = rr;
         lu.solve(dF1.data());
-        gmres(M, Ed, lu, rre, rim, dF2, dF3, res);
+        if (complex_direct) {
+          for (int i = 0; i < n; ++i) cb[i] = std::complex<double>(rre[i], rim[i]);
+          clu.solve(cb.data());
+          for (int i = 0; i < n; ++i) {
+            dF2[i] = cb[i].real();
+            dF3[i] = cb[i].imag();
+          }
+        } else {
+          gmres(M, Ed, lu, rre, rim, dF2, dF3, res);
+        }
         newt++;
         res.newton++;
         double dsq = 0.0;
@@ -1488,7 +1513,7 @@ struct Pipeline {
         gs.data[p] = (Dinv[i] * M.data[p]) * Dinv[M.indices[p]];
     Vec bsc(N);
     for (int i = 0; i < N; ++i) bsc[i] = Dinv[i] * proj[i];
-    Vec c = (opt.nnls_exact || opt.disc == 1) ? nnls_exact(gs, bsc, &admm_iters)
+    Vec c = opt.nnls_exact ? nnls_exact(gs, bsc, &admm_iters)
                                               : nnls_admm(gs, bsc, &admm_iters);
     q0.assign(N, 0.0);
     for (int i = 0; i < N; ++i) {
@@ -1539,7 +1564,7 @@ struct Pipeline {
       }
     Vec y0(N);
     for (int i = 0; i < N; ++i) y0[i] = D[i] * q0[i];
-    RadauSolver rs{opt.rtol, opt.atol, h.T / 5.0, 1e-6, true};
+    RadauSolver rs{opt.rtol, opt.atol, h.T / 5.0, 1e-6, true, opt.complex_direct};
     sol = rs.solve(Ms, Ks, y0, h.T);
     traj.clear();
     for (auto& yy : sol.y) {

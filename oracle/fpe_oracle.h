@@ -35,6 +35,7 @@ typedef struct OrcOptions {
     double ic_sigma_v;     /* config disc IC width in v (<=0 -> 0.004) */
     int32_t nnls_exact;    /* 1: solve the IC NNLS to optimality instead of ADMM */
     int32_t ic_sub;        /* config disc: IC quadrature subintervals per span (<=0 -> 8) */
+    int32_t complex_direct; /* 1: exact complex stage solve instead of GMRES(10) */
 } OrcOptions;
 
 /* ComputePipeline(fp, num_insert) (reference src/server/compute_pipeline.mojo:29-48).

@@ -28,6 +28,7 @@ class OrcOptions(C.Structure):
         ("ic_sigma_v", C.c_double),
         ("nnls_exact", C.c_int32),
         ("ic_sub", C.c_int32),
+        ("complex_direct", C.c_int32),
     ]
 
 
@@ -88,8 +89,9 @@ def _dp(a: np.ndarray):
 
 
 def options(disc=0, num_insert=0, rtol=0.0, atol=0.0, ic_sigma_s=0.0, ic_sigma_v=0.0,
-            nnls_exact=0, ic_sub=0) -> OrcOptions:
-    return OrcOptions(disc, num_insert, rtol, atol, ic_sigma_s, ic_sigma_v, nnls_exact, ic_sub)
+            nnls_exact=0, ic_sub=0, complex_direct=0) -> OrcOptions:
+    return OrcOptions(disc, num_insert, rtol, atol, ic_sigma_s, ic_sigma_v, nnls_exact, ic_sub,
+                      complex_direct)
 
 
 _ARRAYS = {"s_knots": 0, "v_knots": 1, "s": 2, "v": 3, "s_weights": 4, "v_weights": 5,
