@@ -426,7 +426,9 @@ class BatchOptions:
     disc: int = 0            # 0 reference discretization, 1 config discretization
     precision: int = 0       # 0 FP64 factors, 1 FP32 factors + FP64 refinement
     num_insert: int = 50
-    refine: int = 2
+    refine: int = 0          # extra FP64 refinement sweeps per stage solve
+    complex_solve: int = 0   # 0 auto, 1 GMRES(10) (reference algorithm), 2 direct complex LU
+    radau_constants: int = 0  # 0 auto, 1 the reference's U1/ALPH/BETA/TI13, 2 exact Radau IIA
     rtol: float = 1e-4
     atol: float = 1e-6
     ic_sigma_s: float = 0.6
@@ -444,6 +446,8 @@ class BatchOptions:
         o.ic_sigma_s, o.ic_sigma_v, o.ic_sub = self.ic_sigma_s, self.ic_sigma_v, self.ic_sub
         o.greeks = 1 if self.greeks else 0
         o.rel_s, o.rel_v = self.rel_s, self.rel_v
+        o.complex_solve = self.complex_solve
+        o.radau_constants = self.radau_constants
         return o
 
 

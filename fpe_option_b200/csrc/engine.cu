@@ -99,7 +99,9 @@ bool pricing_valid(const Pricing& p, const double* K) {
 }
 
 struct Opts {
-  int disc = 0, precision = 0, num_insert = 50, refine = 2, ic_sub = 8, greeks = 0;
+  int disc = 0, precision = 0, num_insert = 50, refine = 0, ic_sub = 8, greeks = 0;
+  int complex_mode = 0;  // resolved: 0 GMRES(10) (reference), 1 direct complex block LU
+  int radau_exact = 0;   // resolved: 0 the reference's stage constants, 1 exact Radau IIA
   double rtol = 1e-4, atol = 1e-6, ic_sigma_s = 0.6, ic_sigma_v = 0.004, rel_s = 0.01,
          rel_v = 0.1;
 };
@@ -112,6 +114,12 @@ Opts opts_from(const FpeBatchOptions* o, int default_num_insert) {
   r.precision = o->precision;
   if (o->num_insert > 0) r.num_insert = o->num_insert;
   if (o->refine > 0) r.refine = o->refine;
+  // complex_solve: 0 auto (GMRES for the reference discretization, direct
+  // for the config discretization), 1 GMRES(10), 2 direct complex LU
+  r.complex_mode = o->complex_solve == 2 ? 1 : o->complex_solve == 1 ? 0 : (o->disc == 1 ? 1 : 0);
+  // radau_constants: 0 auto (reference values on the reference discretization,
+  // exact Radau IIA on the config discretization), 1 reference, 2 exact
+  r.radau_exact = o->radau_constants == 2 || (o->radau_constants == 0 && o->disc == 1);
   if (o->rtol > 0) r.rtol = o->rtol;
   if (o->atol > 0) r.atol = o->atol;
   if (o->ic_sigma_s > 0) r.ic_sigma_s = o->ic_sigma_s;
@@ -220,21 +228,23 @@ struct FpePlan {
 static int plan_layout(FpePlan* P, int esz) {
   int64_t od = 0, oi = 0, of = 0, ot = 0;
   size_t smem_max = 0;
+  const int cplx = P->o.complex_mode;
   for (auto& d : P->descs) {
     d.off_d = od;
     d.off_i = oi;
     d.off_f = of;
     od += fpe_dlayout(d).total;
     oi += fpe_ilayout(d).total;
-    of += fpe_factor_bytes(d, esz, 0);
+    of += fpe_factor_bytes(d, esz, cplx);
     if (d.save_traj) {
       d.off_traj = ot;
       ot += d.traj_cap + int64_t(d.traj_cap) * d.cap_dof_s * d.cap_dof_v;
     }
     const int nv = std::min(d.cap_dof_v, FPE_MAX_NDOF_V);
     const int ns_cap = std::min(d.cap_dof_s, FPE_MAX_NDOF_S);
-    size_t sm = sizeof(fpe::RadauSmem) + size_t(4 * ns_cap * 7 + 9 * nv * 7) * 8 +
-                size_t(std::max(3 * nv * nv, 2 * nv * nv + 6 * nv)) * esz + 64;
+    const int ebytes = cplx ? 2 * esz : esz;  // the complex factor needs the larger scratch
+    size_t sm = sizeof(fpe::RadauSmem) + size_t(4 * ns_cap * 7 + 5 * nv * 7) * 8 +
+                size_t(std::max(3 * nv * nv, 2 * nv * nv + 6 * nv)) * ebytes + 64;
     smem_max = std::max(smem_max, sm);
   }
   P->n_d = od;
@@ -285,11 +295,14 @@ static int plan_launch(FpePlan* P, cudaStream_t s, int from, int to) {
     ++launches;
   }
   if (from <= 3 && to > 3) {
+    const fpe::RadauConstants rk = fpe::radau_constants(P->o.radau_exact != 0);
     if (P->o.precision == 0) {
-      fpe::RadauKernelArgs<double> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena, P->d_traj, 0};
+      fpe::RadauKernelArgs<double> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena,
+                                     P->d_traj, 0, P->o.complex_mode, rk.u1, rk.alph, rk.beta, rk.ti13};
       fpe::k_radau<double><<<grid, block, P->radau_smem, s>>>(a);
     } else {
-      fpe::RadauKernelArgs<float> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena, P->d_traj, P->o.refine};
+      fpe::RadauKernelArgs<float> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena,
+                                    P->d_traj, P->o.refine, P->o.complex_mode, rk.u1, rk.alph, rk.beta, rk.ti13};
       fpe::k_radau<float><<<grid, block, P->radau_smem, s>>>(a);
     }
     ++launches;

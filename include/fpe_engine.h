@@ -151,12 +151,19 @@ typedef struct FpeBatchOptions {
     int32_t disc;        /* 0 reference discretization, 1 config discretization */
     int32_t precision;   /* 0 FP64 stage factors, 1 FP32 factors + FP64 refinement */
     int32_t num_insert;  /* reference discretization grid size (<= 0 -> 50) */
-    int32_t refine;      /* refinement sweeps in precision 1 (< 0 -> 2, 0 -> 2) */
+    int32_t refine;      /* extra FP64 refinement sweeps per stage solve (<= 0 -> none:
+                            the simplified Newton iteration's FP64 residual refines) */
     double rtol, atol;   /* Radau tolerances (<= 0 -> 1e-4 / 1e-6) */
     double ic_sigma_s, ic_sigma_v; /* config IC widths (<= 0 -> 0.6 / 0.004) */
     int32_t ic_sub;      /* config IC quadrature subintervals per span (<= 0 -> 8) */
     int32_t greeks;      /* 1: delta/gamma/vega by 4 bumped solves per contract */
     double rel_s, rel_v; /* Greeks bumps relative to S0 / V0 (<= 0 -> 0.01 / 0.1) */
+    int32_t complex_solve; /* complex Radau stage: 0 auto (GMRES(10) for disc 0, direct
+                              for disc 1), 1 GMRES(10) with the real-stage preconditioner
+                              (the reference algorithm), 2 direct complex block LU */
+    int32_t radau_constants; /* Radau IIA stage constants: 0 auto (the reference's
+                                U1/ALPH/BETA/TI13 for disc 0, exact for disc 1),
+                                1 the reference's, 2 exact (order-5 Radau IIA) */
 } FpeBatchOptions;
 
 /** Status codes written per strike slot of a batch. */

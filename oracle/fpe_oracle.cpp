@@ -436,6 +436,7 @@ struct Options {
   bool nnls_exact = false;
   int ic_sub = 8;
   bool complex_direct = false;
+  bool radau_exact = false;
 };
 
 static Options options_from(const OrcOptions* o, int default_num_insert) {
@@ -451,6 +452,8 @@ static Options options_from(const OrcOptions* o, int default_num_insert) {
   r.nnls_exact = o->nnls_exact != 0;
   if (o->ic_sub > 0) r.ic_sub = o->ic_sub;
   r.complex_direct = o->complex_direct != 0;
+  // 0 auto: reference constants on the reference discretization, exact on config
+  r.radau_exact = o->radau_constants == 2 || (o->radau_constants == 0 && o->disc == 1);
   return r;
 }
 
@@ -973,6 +976,23 @@ struct RadauSolver {
   double rtol, atol, max_step, first_step;
   bool save_all = true;
   bool complex_direct = false;  // exact complex stage solve instead of GMRES(10)
+  // Eigenvalues of the Radau IIA A^-1 used in the transformed stage equations.
+  // The reference hard-codes U1 = 3.6378165692476072, ALPH = 2.6753213032678365,
+  // BETA = 3.0493570545593676 (radau.mojo:64-66); the exact values (RADCOR:
+  // U1 = 30/(6 + 81^(1/3) - 9^(1/3)), ALPH/BETA from (12 - 81^(1/3) + 9^(1/3))/60
+  // and (81^(1/3) + 9^(1/3)) sqrt(3)/60 over their squared modulus) are
+  // 3.6378342527444962, 2.6810828736277523, 3.0504301992474105.  Because the
+  // constants enter the Newton residual, the reference values integrate a
+  // perturbed, low-order method; set_exact() selects true Radau IIA.  The
+  // reference's TI13 = 0.54177705399358748719 (radau.mojo:75) also transposes
+  // digits of inv(T)[0][2] = 0.54177053993587487119; exact mode corrects it.
+  double U1 = rc::U1, ALPH = rc::ALPH, BETA = rc::BETA, TI13 = rc::TI13;
+  void set_exact() {
+    U1 = 3.6378342527444962;
+    ALPH = 2.6810828736277523;
+    BETA = 3.0504301992474105;
+    TI13 = 0.54177053993587487119;
+  }
 
   // radau.mojo:882-1146 left-preconditioned GMRES on the real 2n form of
   // (ALPH + i BETA) M + h_lu K with P = diag(E1, E1).
@@ -1565,6 +1585,7 @@ struct Pipeline {
     Vec y0(N);
     for (int i = 0; i < N; ++i) y0[i] = D[i] * q0[i];
     RadauSolver rs{opt.rtol, opt.atol, h.T / 5.0, 1e-6, true, opt.complex_direct};
+    if (opt.radau_exact) rs.set_exact();
     sol = rs.solve(Ms, Ks, y0, h.T);
     traj.clear();
     for (auto& yy : sol.y) {
@@ -2090,7 +2111,8 @@ int32_t orc_payoff(int32_t type, const double* K, int32_t nK, double barrier, do
 }
 
 int32_t orc_radau_dense(int32_t n, const double* M, const double* K, const double* y0, double t1,
-                        double rtol, double atol, double max_step, double first_step, double* y_out) {
+                        double rtol, double atol, double max_step, double first_step,
+                        int32_t exact_constants, double* y_out) {
   CSR Mc, Kc;
   Mc.nrows = Mc.ncols = Kc.nrows = Kc.ncols = n;
   Mc.indptr.assign(n + 1, 0);
@@ -2105,6 +2127,7 @@ int32_t orc_radau_dense(int32_t n, const double* M, const double* K, const doubl
     Mc.indptr[i + 1] = Kc.indptr[i + 1] = (i + 1) * n;
   }
   RadauSolver rs{rtol, atol, max_step, first_step, false};
+  if (exact_constants) rs.set_exact();
   RadauResult r = rs.solve(Mc, Kc, Vec(y0, y0 + n), t1);
   std::memcpy(y_out, r.y.back().data(), sizeof(double) * n);
   return r.success ? int32_t(r.accepted) : -1;

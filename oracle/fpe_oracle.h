@@ -36,6 +36,8 @@ typedef struct OrcOptions {
     int32_t nnls_exact;    /* 1: solve the IC NNLS to optimality instead of ADMM */
     int32_t ic_sub;        /* config disc: IC quadrature subintervals per span (<=0 -> 8) */
     int32_t complex_direct; /* 1: exact complex stage solve instead of GMRES(10) */
+    int32_t radau_constants; /* 0 auto (reference for disc 0, exact for disc 1),
+                                1 the reference's U1/ALPH/BETA, 2 exact Radau IIA */
 } OrcOptions;
 
 /* ComputePipeline(fp, num_insert) (reference src/server/compute_pipeline.mojo:29-48).
@@ -110,10 +112,12 @@ int32_t orc_generate_knots(int32_t n, int32_t degree, int32_t nonuniform, double
                            double b0, double b1, double mean, double std_, double* out);
 int32_t orc_payoff(int32_t option_type, const double* K, int32_t nK, double barrier,
                    double S, double* out);
-/* Radau IIA on M y' = -K y with dense M, K (n x n row-major); returns accepted steps. */
+/* Radau IIA on M y' = -K y with dense M, K (n x n row-major); returns accepted
+ * steps (-1 on failure).  exact_constants selects the true Radau IIA eigenvalues
+ * instead of the reference's hard-coded U1/ALPH/BETA. */
 int32_t orc_radau_dense(int32_t n, const double* M, const double* K, const double* y0,
                         double t1, double rtol, double atol, double max_step,
-                        double first_step, double* y_out);
+                        double first_step, int32_t exact_constants, double* y_out);
 
 #ifdef __cplusplus
 }

@@ -29,6 +29,7 @@ class OrcOptions(C.Structure):
         ("nnls_exact", C.c_int32),
         ("ic_sub", C.c_int32),
         ("complex_direct", C.c_int32),
+        ("radau_constants", C.c_int32),
     ]
 
 
@@ -79,7 +80,7 @@ def lib():
         L.orc_payoff.restype = i32
         L.orc_payoff.argtypes = [i32, dp, i32, d, d, dp]
         L.orc_radau_dense.restype = i32
-        L.orc_radau_dense.argtypes = [i32, dp, dp, dp, d, d, d, d, d, dp]
+        L.orc_radau_dense.argtypes = [i32, dp, dp, dp, d, d, d, d, d, i32, dp]
         _lib = L
     return _lib
 
@@ -89,9 +90,9 @@ def _dp(a: np.ndarray):
 
 
 def options(disc=0, num_insert=0, rtol=0.0, atol=0.0, ic_sigma_s=0.0, ic_sigma_v=0.0,
-            nnls_exact=0, ic_sub=0, complex_direct=0) -> OrcOptions:
+            nnls_exact=0, ic_sub=0, complex_direct=0, radau_constants=0) -> OrcOptions:
     return OrcOptions(disc, num_insert, rtol, atol, ic_sigma_s, ic_sigma_v, nnls_exact, ic_sub,
-                      complex_direct)
+                      complex_direct, radau_constants)
 
 
 _ARRAYS = {"s_knots": 0, "v_knots": 1, "s": 2, "v": 3, "s_weights": 4, "v_weights": 5,
@@ -213,11 +214,11 @@ def payoff(option_type, K, barrier, S) -> np.ndarray:
     return out
 
 
-def radau_dense(M, K, y0, t1, rtol, atol, max_step=0.0, first_step=0.0):
+def radau_dense(M, K, y0, t1, rtol, atol, max_step=0.0, first_step=0.0, exact=False):
     M = np.ascontiguousarray(M, np.float64)
     K = np.ascontiguousarray(K, np.float64)
     y0 = np.ascontiguousarray(y0, np.float64)
     out = np.empty_like(y0)
     n = lib().orc_radau_dense(len(y0), _dp(M), _dp(K), _dp(y0), t1, rtol, atol, max_step,
-                              first_step, _dp(out))
+                              first_step, int(exact), _dp(out))
     return out, n
