@@ -1,0 +1,333 @@
+"""Benchmark: FPE option prices/sec on B200 (batched, mixed precision).
+
+Workload (one "step" = pricing one batch): 256 European Heston contracts drawn
+from a fixed seed with kappa~U[0.5,3], theta~U[0.02,0.15], eta~U[0.1,0.8],
+rho~U[-0.9,0], V0~U[0.02,0.2], r~U[0,0.05], T~U[0.1,2], S0=100,
+K/S0~U[0.8,1.2], calls/puts 50/50, grids n_s in {32,48,64} x n_v in {16,24,32}
+(sinh-stretched clamped cubic B-splines, s_max = 3 S0, v_max = 1), solved in
+one launch sequence with FP32 stage factors + FP64 Newton residuals, direct
+complex stage solve and exact Radau IIA constants.  Synthetic data (no public
+dataset is involved).  Each rank prices its own batch (seed + rank): weak
+scaling, no data-path collective.
+
+value: prices/s with the contract descriptors resident in HBM, device time
+of the five kernels (CUDA events on the launching stream), max over ranks.
+e2e:   prices/s through the public C ABI from host contracts to host prices
+(plan creation with its host-to-device copy, kernels, device-to-host copy).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FPE option prices/sec on 1 B200 at <=1e-4 rel err: batched vs plain vs surrogate"
+N_CONTRACTS = 256
+RTOL = 1e-6  # Radau tolerance of the batched run (atol = rtol * 1e-2)
+REF_RTOL = 1e-10  # FP64 reference run used to state the error
+
+
+def make_batch(n: int, seed: int):
+    """Config-1 parameter draws: (n, 12) float + (n, 3) int tables."""
+    rng = np.random.default_rng(seed)
+    P = np.zeros((n, 12))
+    I = np.zeros((n, 3), np.int32)
+    for j in range(n):
+        P[j] = [rng.uniform(0.5, 3), rng.uniform(0.02, 0.15), rng.uniform(0.1, 0.8),
+                rng.uniform(-0.9, 0), rng.uniform(0, 0.05), rng.uniform(0.1, 2), 100.0,
+                rng.uniform(0.02, 0.2), 100.0 * rng.uniform(0.8, 1.2), 0.0, 0.0, 300.0]
+        I[j] = [rng.choice([32, 48, 64]), rng.choice([16, 24, 32]), 8 if j % 2 == 0 else 9]
+    return P, I
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of k_radau from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", "k_radau_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device),
+                                      f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout
+                for line in out.strip().splitlines():
+                    self.rows.append([c.strip() for c in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_run(P, I, rtol, n_threads, sample):
+    """The oracle port (single-threaded per solve, solves spread over threads)."""
+    from oracle import pyoracle as po
+
+    opt = po.options(disc=1, rtol=rtol, atol=rtol * 1e-2)
+    idx = np.arange(sample)
+    t = time.perf_counter()
+    po.price_batch(P[idx], I[idx], opt, n_threads=n_threads)
+    dt = time.perf_counter() - t
+    return sample / dt, dt
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    P, I = make_batch(N_CONTRACTS, args.seed)
+    cores = os.cpu_count() or 1
+    sample = max(cores, min(args.cpu_sample, N_CONTRACTS))
+    rates = []
+    for _ in range(args.warmup):
+        cpu_baseline_run(P, I, args.rtol, cores, min(sample, cores))
+    for s in range(args.steps):
+        sl = (np.arange(sample) + s * sample) % N_CONTRACTS
+        r, _ = cpu_baseline_run(P[sl], I[sl], args.rtol, cores, sample)
+        rates.append(r)
+    v = float(np.mean(rates))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "prices/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * sample / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "config1 256 European contracts, mixed grids",
+                       "rtol": args.rtol, "contracts_per_step": sample},
+            "cpu_baseline": {"value": v, "unit": "prices/s", "cores": cores, "kind": "port",
+                             "sample": f"{sample} contracts of the config-1 batch per step, "
+                                       f"oracle C++ FP64 restatement, {cores} threads"},
+            "e2e": {"value": v, "unit": "prices/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--rtol", type=float, default=RTOL)
+    ap.add_argument("--precision", type=int, default=1)
+    ap.add_argument("--cpu-sample", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from fpe_option_b200 import build
+
+    if rank == 0:
+        build.build_library()
+    if world > 1:
+        dist.barrier()
+    import fpe_option_b200 as fpe
+
+    if not fpe.is_available():
+        raise RuntimeError("CUDA engine unavailable")
+    P, I = make_batch(N_CONTRACTS, args.seed + rank)
+    opts = fpe.BatchOptions(disc=1, precision=args.precision, rtol=args.rtol,
+                            atol=args.rtol * 1e-2, complex_solve=2, radau_constants=2)
+    arr, keep = fpe.contracts_from_arrays(P, I)
+    plan = fpe.Plan(arr, opts, _keep=keep)
+    # a dedicated (non-default) stream: the kernels and the timing events share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sptr = stream.cuda_stream
+    assert sptr != 0
+    # accuracy: the same batch in FP64 at a tight tolerance (untimed)
+    ref = fpe.Plan(arr, fpe.BatchOptions(disc=1, precision=0, rtol=REF_RTOL,
+                                         atol=REF_RTOL * 1e-2, complex_solve=2,
+                                         radau_constants=2), _keep=keep)
+    ref.run()
+    p_ref, _, _, _, st_ref = ref.results()
+    ref.close()
+    for _ in range(max(args.warmup, 3)):
+        plan.run(sptr)
+    torch.cuda.synchronize()
+    p_out, _, _, _, st = plan.results()
+    floor = 1e-6 * 100.0
+    rel = np.abs(p_out - p_ref) / np.maximum(np.abs(p_ref), floor)
+    rel_unfloored = np.abs(p_out - p_ref) / np.abs(p_ref)
+    # per-kernel times and the roofline of the dominant kernel (k_radau)
+    ktimes = plan.kernel_times(sptr)
+    stats = plan.stats()
+    # ---- device-resident timed region ------------------------------------------
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.run(sptr)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * N_CONTRACTS * args.steps / (ms / 1000.0)
+    # ---- end to end through the public C ABI (host contracts -> host prices) -----
+    pinned = torch.empty((N_CONTRACTS, 12), dtype=torch.float64).pin_memory()
+    pinned.copy_(torch.from_numpy(P))
+    Ph = pinned.numpy()
+    h2d = N_CONTRACTS * (C_SIZE_CONTRACT()) + N_CONTRACTS * 8
+    d2h = N_CONTRACTS * 8 + stats["solves"] * 80
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        a2, k2 = fpe.contracts_from_arrays(Ph, I)
+        pl = fpe.Plan(a2, opts, _keep=k2)
+        pl.run(sptr)
+        pe, _, _, _, _ = pl.results()
+        pl.close()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * N_CONTRACTS * args.steps / e2e_s
+    # ---- roofline of k_radau -----------------------------------------------------
+    peak, peak_kind = load_peaks()
+    radau_ms = ktimes[3]
+    achieved = stats["factor_bytes"] / (radau_ms / 1000.0) / 1e9
+    traffic = load_traffic()
+    # ---- CPU baseline (oracle port), rank 0, bounded sample -------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        sample = max(min(cores, N_CONTRACTS), min(args.cpu_sample, N_CONTRACTS))
+        rate, dt = cpu_baseline_run(P, I, args.rtol, cores, sample)
+        cpu = {"value": rate, "unit": "prices/s", "cores": cores, "kind": "port",
+               "sample": f"first {sample} contracts of the same batch, oracle C++ FP64 "
+                         f"restatement on {cores} host threads, {dt:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "prices/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32-factors/f64" if args.precision == 1 else "f64", "data": "synthetic",
+            "config": {"workload": "config1: 256 European Heston contracts per GPU, mixed grids "
+                                   "32-64 x 16-32, one launch sequence",
+                       "rtol": args.rtol, "atol": args.rtol * 1e-2, "precision": args.precision,
+                       "complex_stage": "direct block LU", "radau_constants": "exact",
+                       "l2": "inputs and factors larger than L2 (126 MB)",
+                       "max_rel_err_vs_fp64": float(rel.max()), "err_floor": floor,
+                       "max_rel_err_unfloored": float(rel_unfloored.max()),
+                       "fp64_reference_rtol": REF_RTOL,
+                       "status_ok": bool((st == 0).all() and (st_ref == 0).all())},
+            "e2e": {"value": e2e, "unit": "prices/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": 5 * args.steps,
+            "kernel_ms": {"setup": ktimes[0], "galerkin": ktimes[1], "ic": ktimes[2],
+                          "radau": ktimes[3], "payoff": ktimes[4]},
+            "solver": {k: int(v) for k, v in stats.items()},
+            "roofline": {"bound": "hbm", "kernel": "k_radau", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind,
+                         "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                         "algorithmic_bytes": int(stats["factor_bytes"])},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def C_SIZE_CONTRACT():
+    import ctypes
+
+    from fpe_option_b200 import _lib
+
+    return ctypes.sizeof(_lib.FpeContract)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -504,11 +504,20 @@ class Plan:
         return p, dl, g, v, st
 
     def stats(self) -> dict:
-        out = (C.c_int64 * 10)()
+        out = (C.c_int64 * 16)()
         self._L.fpe_plan_stats(self._h, out)
         keys = ["solves", "accepted", "rejected", "newton", "gmres", "lu", "admm",
-                "max_ndof_s", "max_ndof_v", "total_dofs"]
+                "max_ndof_s", "max_ndof_v", "total_dofs", "passes_real", "passes_complex",
+                "factor_bytes", "worst_status"]
         return dict(zip(keys, list(out)))
+
+    def kernel_times(self, stream: int | None = None) -> list[float]:
+        """Run once with CUDA events around each kernel; returns ms for
+        [setup, galerkin, ic, radau, payoff]."""
+        ms = (C.c_float * 5)()
+        if self._L.fpe_plan_kernel_times(self._h, C.c_void_p(stream) if stream else None, ms) < 0:
+            raise RuntimeError("fpe_plan_kernel_times failed")
+        return list(ms)
 
     def close(self):
         if getattr(self, "_h", None):

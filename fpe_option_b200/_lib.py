@@ -65,6 +65,7 @@ EXPORTED = [
     "fpe_compute_free_oneshot", "fpe_plan_create", "fpe_plan_run", "fpe_plan_results",
     "fpe_plan_stats", "fpe_plan_sizes", "fpe_plan_destroy", "fpe_price_batch",
     "fpe_compute_create_ex", "fpe_compute_basis_csr", "fpe_device_available",
+    "fpe_plan_kernel_times",
 ]
 
 _lib = None
@@ -109,6 +110,8 @@ def load():
     L.fpe_plan_results.argtypes = [cp, dp, dp, dp, dp, ip]
     L.fpe_plan_stats.restype = i32
     L.fpe_plan_stats.argtypes = [cp, C.POINTER(C.c_int64)]
+    L.fpe_plan_kernel_times.restype = i32
+    L.fpe_plan_kernel_times.argtypes = [cp, vp, C.POINTER(C.c_float)]
     L.fpe_plan_sizes.restype = i32
     L.fpe_plan_sizes.argtypes = [cp, ip, ip]
     L.fpe_plan_destroy.argtypes = [cp]

@@ -690,7 +690,7 @@ int32_t fpe_plan_results(FpePlan* P, double* prices, double* delta, double* gamm
 int32_t fpe_plan_stats(FpePlan* P, int64_t* out) {
   if (!P || !out) return -1;
   if (plan_fetch(P) < 0) return -1;
-  for (int k = 0; k < 10; ++k) out[k] = 0;
+  for (int k = 0; k < 16; ++k) out[k] = 0;
   out[0] = int64_t(P->descs.size());
   for (size_t s = 0; s < P->descs.size(); ++s) {
     const int32_t* in = &P->h_infos[s * FPE_INFO_COUNT];
@@ -703,8 +703,40 @@ int32_t fpe_plan_stats(FpePlan* P, int64_t* out) {
     out[7] = std::max<int64_t>(out[7], in[FPE_INFO_NDOF_S]);
     out[8] = std::max<int64_t>(out[8], in[FPE_INFO_NDOF_V]);
     out[9] += int64_t(in[FPE_INFO_NDOF_S]) * in[FPE_INFO_NDOF_V];
+    // algorithmic stage-factor bytes: each LU writes R (+ C) once, each sweep
+    // reads the whole real (R) or complex (C = 2R) factor once
+    const int64_t nv = in[FPE_INFO_NDOF_V], ns = in[FPE_INFO_NDOF_S];
+    const int64_t R = ns * 7 * nv * nv * (P->o.precision == 0 ? 8 : 4);
+    const int64_t Cb = P->o.complex_mode ? 2 * R : 0;
+    out[10] += in[FPE_INFO_PASS_REAL];
+    out[11] += in[FPE_INFO_PASS_CPLX];
+    out[12] += int64_t(in[FPE_INFO_PASS_REAL]) * R + int64_t(in[FPE_INFO_PASS_CPLX]) * Cb +
+               int64_t(in[FPE_INFO_LU]) * (R + Cb);
+    out[13] = std::max<int64_t>(out[13], in[FPE_INFO_STATUS]);
   }
   return 0;
+}
+
+int32_t fpe_plan_kernel_times(FpePlan* P, void* stream, float* ms) {
+  if (!P || !ms) return -1;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P->stream;
+  cudaEvent_t ev[6];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  if (s != P->stream) {
+    CK(cudaEventRecord(ev[0], P->stream));
+    CK(cudaStreamWaitEvent(s, ev[0], 0));
+  }
+  P->fetched = false;
+  for (int k = 0; k < 5; ++k) {
+    CK(cudaEventRecord(ev[k], s));
+    if (plan_launch(P, s, k, k + 1) < 0) return -1;
+  }
+  CK(cudaEventRecord(ev[5], s));
+  CK(cudaEventSynchronize(ev[5]));
+  for (int k = 0; k < 5; ++k) CK(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+  for (auto& e : ev) cudaEventDestroy(e);
+  P->ran = true;
+  return 5;
 }
 
 int32_t fpe_plan_sizes(FpePlan* P, int32_t* n_results, int32_t* n_solves) {

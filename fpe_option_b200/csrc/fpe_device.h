@@ -29,7 +29,7 @@ enum FpeInfo {
   FPE_INFO_NKNOT_S, FPE_INFO_NKNOT_V, FPE_INFO_NGRID_S, FPE_INFO_NGRID_V,
   FPE_INFO_NQ_S, FPE_INFO_NQ_V, FPE_INFO_NDOF_S, FPE_INFO_NDOF_V,
   FPE_INFO_ACCEPTED, FPE_INFO_REJECTED, FPE_INFO_NEWTON, FPE_INFO_GMRES, FPE_INFO_LU,
-  FPE_INFO_ADMM, FPE_INFO_REFINE, FPE_INFO_NSAVED,
+  FPE_INFO_ADMM, FPE_INFO_PASS_REAL, FPE_INFO_NSAVED, FPE_INFO_PASS_CPLX,
   FPE_INFO_COUNT = 20
 };
 

@@ -205,7 +205,10 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
   const double* Dvv = D + DL.D_v;
 
   // block solves ------------------------------------------------------------
+  long n_pass_r = 0, n_pass_c = 0;  // sweeps over the real / complex factors
   auto solve_set = [&](double* xr0, double* xr1, int nr, double* xc_re, double* xc_im, int nc) {
+    n_pass_r += nr > 0;
+    n_pass_c += nc > 0;
     SolveSet<FT> Sv;
     Sv.R = &LR;
     Sv.Cf = &LC;
@@ -649,6 +652,8 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
     info[FPE_INFO_GMRES] = int(n_gmres);
     info[FPE_INFO_LU] = int(n_lu);
     info[FPE_INFO_NSAVED] = n_saved;
+    info[FPE_INFO_PASS_REAL] = int(n_pass_r);
+    info[FPE_INFO_PASS_CPLX] = int(n_pass_c);
   }
 }
 

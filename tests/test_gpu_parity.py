@@ -1,0 +1,247 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU FP64 oracle
+and the committed golden fixtures.  Marked gpu; run on a B200 with -m gpu.
+
+Tolerances: the reference-parity mode (reference discretization, GMRES(10)
+complex stage, the reference's Radau constants, FP64 factors) matches the
+oracle to 1e-9 relative; FP32 factors (precision 1) to 1e-6; the direct
+complex stage solve to 1e-6 at tight tolerances.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "oracle_golden.json")
+H = dict(kappa=1.2, theta=0.05, sigma=0.35, rho=-0.4, r=0.1, T=0.6, S0=60.0, V0=0.1)
+
+
+def _plan_prices(fpe, args, opts):
+    K = args["K"]
+    n = len(K)
+    p = np.zeros((n, 12))
+    i = np.zeros((n, 3), np.int32)
+    for j, k in enumerate(K):
+        p[j] = [args["kappa"], args["theta"], args["sigma"], args["rho"], args["r"], args["T"],
+                args["S0"], args["V0"], k, args.get("barrier", 0.0), args.get("s_min", 0.0),
+                args.get("s_max", -1.0)]
+        i[j] = [args["n_s"], args["n_v"], args["option_type"]]
+    prices, status = fpe.price_batch(p, i, opts)
+    return prices, status
+
+
+def _golden():
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-9), (1, 1e-4)])
+def test_golden_reference_cases(engine, precision, tol):
+    """Reference discretization at the reference Pricer tolerances (rtol 1e-4):
+    FP64 factors reproduce the oracle to 1e-9, FP32 factors to the stated 1e-4."""
+    fpe = engine
+    for case in _golden()["small_cases"]:
+        o = case.get("options", {})
+        if o.get("disc", 0) != 0:
+            continue
+        opts = fpe.BatchOptions(num_insert=o.get("num_insert", 50), precision=precision,
+                                complex_solve=1, radau_constants=1)
+        got, st = _plan_prices(fpe, case["args"], opts)
+        assert (st == 0).all()
+        exp = np.array(case["prices"])
+        rel = np.abs(got - exp) / np.maximum(np.abs(exp), 1e-8)
+        assert rel.max() < tol, (case["args"], got, exp)
+
+
+@pytest.mark.parametrize("complex_solve,tol", [(1, 1e-9), (2, 1e-6)])
+def test_golden_config_cases(engine, complex_solve, tol):
+    fpe = engine
+    for case in _golden()["small_cases"]:
+        o = case.get("options", {})
+        if o.get("disc", 0) != 1:
+            continue
+        opts = fpe.BatchOptions(disc=1, rtol=o["rtol"], atol=o["atol"], precision=0,
+                                complex_solve=complex_solve, radau_constants=2)
+        got, st = _plan_prices(fpe, case["args"], opts)
+        assert (st == 0).all()
+        exp = np.array(case["prices"])
+        assert (np.abs(got - exp) / np.abs(exp)).max() < tol
+
+
+def test_live_oracle_all_types(engine, oracle):
+    """One contract of every option type, GPU vs the oracle computed now."""
+    fpe = engine
+    for ot, B in [(8, 0.0), (9, 0.0), (2, 52.0), (3, 52.0), (0, 52.0), (1, 52.0), (6, 70.0),
+                  (7, 70.0), (4, 70.0), (5, 70.0)]:
+        args = dict(H, K=[58.0, 62.0], barrier=B, option_type=ot, n_s=9, n_v=9, s_max=160.0)
+        exp = oracle.pricer_price(**args, opt=oracle.options(num_insert=40))
+        got, st = _plan_prices(fpe, args, fpe.BatchOptions(num_insert=40, complex_solve=1,
+                                                           radau_constants=1))
+        assert (st == 0).all()
+        np.testing.assert_allclose(got, exp, rtol=1e-9, atol=1e-12)
+
+
+def test_knock_in_out_parity_is_exact(engine):
+    fpe = engine
+    args = dict(H, K=[60.0, 70.0], n_s=8, n_v=8, s_max=150.0)
+    opts = fpe.BatchOptions(num_insert=50)
+    van, _ = _plan_prices(fpe, dict(args, option_type=8, barrier=0.0), opts)
+    doc, _ = _plan_prices(fpe, dict(args, option_type=2, barrier=50.0), opts)
+    dic, _ = _plan_prices(fpe, dict(args, option_type=0, barrier=50.0), opts)
+    np.testing.assert_allclose(dic + doc, van, rtol=0, atol=1e-14)
+
+
+def test_readme_one_shot_pins(engine):
+    # README.md:380-392 through the drop-in price()
+    fpe = engine
+    r = fpe.price(S0=60.0, V0=0.1, T=0.6, r=0.1, kappa=1.2, theta=0.05, sigma=0.35, rho=-0.4,
+                  n_s=38, n_v=38, K=[80, 90, 100], s_max=150.0, option_type="european_call")
+    np.testing.assert_allclose(r.prices, [0.966276, 0.280919, 0.078883], atol=6e-7)
+    np.testing.assert_allclose(r.deltas, [0.175855, 0.060298, 0.018875], atol=6e-7)
+    np.testing.assert_allclose(r.gammas, [0.017766, 0.009270, 0.002742], atol=6e-7)
+    np.testing.assert_allclose(r.vegas, [14.057144, 6.197252, 2.283113], atol=6e-6)
+    d = fpe.price(S0=60.0, V0=0.1, T=0.6, r=0.1, n_s=38, n_v=38, K=[80, 90, 100], s_max=150.0,
+                  barrier=50.0, option_type="down_and_out_call")
+    np.testing.assert_allclose(d.prices, [0.905038, 0.263874, 0.074223], atol=6e-7)
+
+
+def test_engine_greeks_vs_golden(engine):
+    fpe = engine
+    g = _golden()["engine"]
+    a = g["args"]
+    r = fpe.price(kappa=a["kappa"], theta=a["theta"], sigma=a["sigma"], rho=a["rho"], r=a["r"],
+                  T=a["T"], S0=a["S0"], V0=a["V0"], K=a["K"], barrier=a["barrier"],
+                  option_type=a["option_type"], n_s=a["n_s"], n_v=a["n_v"], s_max=a["s_max"])
+    for key, got in (("prices", r.prices), ("deltas", r.deltas), ("gammas", r.gammas),
+                     ("vegas", r.vegas)):
+        exp = np.array(g[key])
+        assert np.max(np.abs(got - exp) / np.maximum(np.abs(exp), 1e-6)) < 1e-7, key
+
+
+def test_stepwise_intermediates_vs_golden(engine):
+    fpe = engine
+    s = _golden()["stepwise"]
+    kw = dict(s["kwargs"])
+    c = fpe.Compute(**kw)
+    np.testing.assert_allclose(c.knots.s, s["s_knots"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(c.knots.v, s["v_knots"], rtol=0, atol=1e-15)
+    q0 = c.initial_condition
+    np.testing.assert_allclose(q0, s["q0"], rtol=1e-8, atol=1e-10 * np.abs(s["q0"]).max())
+    sol = c.solve
+    assert len(sol) == s["dims"]["accepted"] + 1
+    np.testing.assert_allclose(sol[-1], s["qT"], rtol=1e-8, atol=1e-10 * np.abs(s["qT"]).max())
+    np.testing.assert_allclose(c.payoff_price([100.0]), s["price_100"], rtol=1e-9)
+
+
+def test_stepwise_vs_live_oracle(engine, oracle):
+    fpe = engine
+    kw = dict(H, n_s=10, n_v=9, option_type=2, barrier=55.0, s_max=140.0)
+    c = fpe.Compute(**kw, num_insert=60)
+    o = oracle.Pipeline(**kw, opt=oracle.options(num_insert=60))
+    gp = c.grid_points
+    np.testing.assert_allclose(gp.s, o.array("s"), rtol=0, atol=1e-12)
+    np.testing.assert_allclose(gp.v, o.array("v"), rtol=0, atol=1e-14)
+    np.testing.assert_allclose(gp.s_weights, o.array("s_weights"), rtol=1e-13, atol=1e-15)
+    np.testing.assert_allclose(gp.v_weights, o.array("v_weights"), rtol=1e-13, atol=1e-17)
+    b = c.basis_1d
+    for which, mat in ((0, b.Bs), (1, b.dBs), (2, b.Bv), (3, b.dBv)):
+        data, idx, ptr, shape = o.basis_csr(which)
+        assert mat.shape == shape
+        np.testing.assert_allclose(mat.toarray(), _csr_dense(data, idx, ptr, shape), rtol=1e-12,
+                                   atol=1e-12)
+    pdf = c.pdf
+    np.testing.assert_allclose(pdf.ravel(), o.array("pdf"), rtol=1e-7,
+                               atol=1e-9 * np.abs(pdf).max())
+    np.testing.assert_allclose(c.payoff_price([60.0, 65.0]), o.price_at([60.0, 65.0]), rtol=1e-9)
+
+
+def _csr_dense(data, idx, ptr, shape):
+    import scipy.sparse as sp
+
+    return sp.csr_matrix((data, idx, ptr), shape=shape).toarray()
+
+
+def test_invalid_contract_gives_status(engine, oracle):
+    fpe = engine
+    p = np.array([[1.2, 0.05, 0.35, -0.4, 0.1, 0.6, 60.0, 0.1, 60.0, 70.0, 0.0, 150.0],
+                  [1.2, 0.05, 0.35, -0.4, 0.1, 0.6, 60.0, 0.1, 60.0, 0.0, 0.0, 150.0]])
+    i = np.array([[8, 8, 2], [8, 8, 8]], np.int32)  # DOC with barrier above spot: invalid
+    prices, st = fpe.price_batch(p, i, fpe.BatchOptions(num_insert=30))
+    assert st[0] == 16 and prices[0] == 0.0
+    # the valid neighbour in the same batch is unaffected (the coarse num_insert=30
+    # grid gives the reference's own, inaccurate, value)
+    exp = oracle.pricer_price(*H.values(), K=[60.0], option_type=8, n_s=8, n_v=8, s_max=150.0,
+                              opt=oracle.options(num_insert=30))
+    assert st[1] == 0
+    np.testing.assert_allclose(prices[1], exp[0], rtol=1e-9)
+
+
+def test_mixed_precision_config_batch(engine):
+    """Config discretization, mixed sizes in one launch: FP32 factors + FP64
+    Newton residual agree with the FP64 factors to well below 1e-4."""
+    fpe = engine
+    rng = np.random.default_rng(11)
+    n = 24
+    p = np.zeros((n, 12))
+    i = np.zeros((n, 3), np.int32)
+    for j in range(n):
+        p[j] = [rng.uniform(0.5, 3), rng.uniform(0.02, 0.15), rng.uniform(0.1, 0.8),
+                rng.uniform(-0.9, 0), rng.uniform(0, 0.05), rng.uniform(0.1, 2), 100.0,
+                rng.uniform(0.02, 0.2), 100 * rng.uniform(0.8, 1.2), 0.0, 0.0, 300.0]
+        i[j] = [rng.choice([16, 24]), rng.choice([12, 16]), rng.choice([8, 9])]
+    o64 = fpe.BatchOptions(disc=1, precision=0, rtol=1e-7, atol=1e-9)
+    o32 = fpe.BatchOptions(disc=1, precision=1, rtol=1e-7, atol=1e-9)
+    p64, s64 = fpe.price_batch(p, i, o64)
+    p32, s32 = fpe.price_batch(p, i, o32)
+    assert (s64 == 0).all() and (s32 == 0).all()
+    rel = np.abs(p32 - p64) / np.maximum(np.abs(p64), 1e-4)
+    assert rel.max() < 1e-6
+
+
+# ---- ported from the reference's tests/test_pricer_stepwise.py ------------------------
+@pytest.fixture
+def ctx(engine):
+    return engine.Compute(S0=60.0, V0=0.1, T=0.6, r=0.1, n_s=8, n_v=8)
+
+
+def test_stepwise_types_and_caching(engine, ctx):
+    from scipy import sparse
+
+    fpe = engine
+    k = ctx.knots
+    assert isinstance(k, fpe.KnotsResult) and k.s.dtype == np.float64 and len(k.v) > 0
+    assert ctx.knots is k
+    gp = ctx.grid_points
+    assert isinstance(gp, fpe.GridPointsResult) and len(gp.s_weights) == len(gp.s)
+    assert np.all(gp.s_weights >= 0.0) and ctx.grid_points is gp
+    b = ctx.basis_1d
+    assert isinstance(b, fpe.Basis1DResult) and isinstance(b.Bs, sparse.csr_matrix)
+    assert b.Bs.shape[0] > 0 and ctx.basis_1d is b
+    assert isinstance(ctx.basis_2d, sparse.csr_matrix) and ctx.basis_2d.shape[0] > 0
+    q0 = ctx.initial_condition
+    assert isinstance(q0, np.ndarray) and q0.dtype == np.float64
+    sol = ctx.solve
+    assert isinstance(sol, list) and len(sol) > 0 and all(t.dtype == np.float64 for t in sol)
+    pdf = ctx.pdf
+    assert pdf.ndim == 2 and pdf.dtype == np.float64
+    p = ctx.payoff_price([80.0, 100.0, 120.0])
+    assert len(p) == 3 and p[0] != p[2]
+    g = ctx.greeks([65.0, 70.0, 75.0, 80.0])
+    assert isinstance(g, fpe.GreeksResult) and g.delta.shape == (4,)
+    assert np.all(ctx.greeks([65.0, 100.0]).delta < 0)
+
+
+def test_stepwise_invalid_and_domain(engine):
+    fpe = engine
+    with pytest.raises(Exception):
+        fpe.Compute(n_s=1)
+    with pytest.raises(Exception):
+        fpe.Compute(option_type="invalid")
+    c = fpe.Compute(S0=60.0, V0=0.1, T=0.6, r=0.1, n_s=8, n_v=8, s_min=10.0, s_max=200.0)
+    assert c.grid_points.s[0] >= 10.0 and c.grid_points.s[-1] <= 200.0
+    pr = fpe.price(S0=60.0, K=50.0, T=0.6, n_s=16, n_v=16, s_min=10.0, s_max=200.0)
+    assert len(pr.prices) == 1 and pr.prices[0] > 0
+    pr = fpe.price(S0=60.0, K=[80.0, 100.0, 120.0], T=0.6, n_s=8, n_v=8)
+    assert len(pr.prices) == 3 and isinstance(pr, fpe.PriceResult)
