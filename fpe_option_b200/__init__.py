@@ -504,11 +504,12 @@ class Plan:
         return p, dl, g, v, st
 
     def stats(self) -> dict:
-        out = (C.c_int64 * 16)()
+        out = (C.c_int64 * 20)()
         self._L.fpe_plan_stats(self._h, out)
         keys = ["solves", "accepted", "rejected", "newton", "gmres", "lu", "admm",
                 "max_ndof_s", "max_ndof_v", "total_dofs", "passes_real", "passes_complex",
-                "factor_bytes", "worst_status"]
+                "factor_bytes", "worst_status", "kcyc_factor", "kcyc_solve", "kcyc_kron",
+                "kcyc_total"]
         return dict(zip(keys, list(out)))
 
     def kernel_times(self, stream: int | None = None) -> list[float]:

@@ -135,125 +135,329 @@ __device__ void blu_assemble(const OpFactors& O, const BlockLU<ET>& L, double a_
   __syncthreads();
 }
 
-// Gauss-Jordan inverse with partial pivoting of the nv x nv block P (global,
-// in place).  aug: nv x 2nv shared ET; aux: 6 nv shared ET.
+// Factorization arithmetic type: the storage type (FP32 factors are computed
+// in FP32, FP64 factors in FP64).
 template <typename ET>
-__device__ bool gj_invert(ET* P, int nv, ET* aug, ET* aux, int* piv_s) {
-  using A = typename AccOf<ET>::T;
-  const int w = 2 * nv;
-  for (int e = threadIdx.x; e < nv * w; e += blockDim.x) {
-    const int r = e / w, c = e - r * w;
-    if (c < nv) aug[e] = P[r * nv + c];
-    else st_elem(aug[e], (c - nv == r) ? aone(A()) : azero(A()));
+struct FacOf;
+template <>
+struct FacOf<float> { using T = float; };
+template <>
+struct FacOf<double> { using T = double; };
+template <>
+struct FacOf<Cx<float>> { using T = Cx<float>; };
+template <>
+struct FacOf<Cx<double>> { using T = Cx<double>; };
+
+__device__ __forceinline__ float fzero(float) { return 0.f; }
+__device__ __forceinline__ double fzero(double) { return 0.0; }
+template <typename T>
+__device__ __forceinline__ Cx<T> fzero(Cx<T>) { return cmk(T(0), T(0)); }
+__device__ __forceinline__ float fone(float) { return 1.f; }
+__device__ __forceinline__ double fone(double) { return 1.0; }
+template <typename T>
+__device__ __forceinline__ Cx<T> fone(Cx<T>) { return cmk(T(1), T(0)); }
+__device__ __forceinline__ void ffma(float& a, float x, float y) { a = fmaf(x, y, a); }
+__device__ __forceinline__ void ffma(double& a, double x, double y) { a = fma(x, y, a); }
+template <typename T>
+__device__ __forceinline__ void ffma(Cx<T>& a, Cx<T> x, Cx<T> y) {
+  a.re = fma(x.re, y.re, fma(-x.im, y.im, a.re));
+  a.im = fma(x.re, y.im, fma(x.im, y.re, a.im));
+}
+__device__ __forceinline__ float fsub(float a, float b) { return a - b; }
+__device__ __forceinline__ double fsub(double a, double b) { return a - b; }
+template <typename T>
+__device__ __forceinline__ Cx<T> fsub(Cx<T> a, Cx<T> b) { return cmk(a.re - b.re, a.im - b.im); }
+__device__ __forceinline__ float fmul(float a, float b) { return a * b; }
+__device__ __forceinline__ double fmul(double a, double b) { return a * b; }
+template <typename T>
+__device__ __forceinline__ Cx<T> fmul(Cx<T> a, Cx<T> b) {
+  return cmk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+__device__ __forceinline__ float finv(float a) { return a != 0.f ? 1.f / a : 0.f; }
+__device__ __forceinline__ double finv(double a) { return a != 0.0 ? 1.0 / a : 0.0; }
+template <typename T>
+__device__ __forceinline__ Cx<T> finv(Cx<T> a) {
+  const T d = a.re * a.re + a.im * a.im;
+  return d != T(0) ? cmk(a.re / d, -a.im / d) : cmk(T(0), T(0));
+}
+__device__ __forceinline__ double fmag(float a) { return fabs(double(a)); }
+__device__ __forceinline__ double fmag(double a) { return fabs(a); }
+template <typename T>
+__device__ __forceinline__ double fmag(Cx<T> a) {
+  return sqrt(double(a.re) * double(a.re) + double(a.im) * double(a.im));
+}
+
+// Shared scratch (in ET elements) needed by blu_factor for block size nv: the
+// augmented pivot block [P | I] (row stride 2 nv + 1), the inverse P^-1, the
+// staged E_{r,i} and U_{i,c} blocks and the computed L_{r,i} blocks, plus the
+// Gauss-Jordan bookkeeping.
+__host__ __device__ __forceinline__ int blu_smem_elems(int nv) {
+  return nv * (2 * nv + 1) + 10 * nv * nv + 4 * nv + 16;
+}
+
+// 2 x 2 register tile of C = A B (nv x nv operands, row strides lda / ldb),
+// rows j0, j0 + 1 and columns l0, l0 + 1 (guarded at odd edges).
+template <typename ET>
+__device__ __forceinline__ void tile2x2(const ET* A_, int lda, const ET* B_, int ldb, int nv, int j0,
+                                        int l0, ET (&acc)[2][2]) {
+  acc[0][0] = acc[0][1] = acc[1][0] = acc[1][1] = fzero(ET());
+  const int j1 = min(j0 + 1, nv - 1), l1 = min(l0 + 1, nv - 1);
+#pragma unroll 4
+  for (int m = 0; m < nv; ++m) {
+    const ET a0 = A_[j0 * lda + m], a1 = A_[j1 * lda + m];
+    const ET b0 = B_[m * ldb + l0], b1 = B_[m * ldb + l1];
+    ffma(acc[0][0], a0, b0);
+    ffma(acc[0][1], a0, b1);
+    ffma(acc[1][0], a1, b0);
+    ffma(acc[1][1], a1, b1);
   }
-  __syncthreads();
-  ET* prow = aux;
-  ET* orow = aux + w;
-  ET* fcol = aux + 2 * w;
-  bool ok = true;
-  for (int c = 0; c < nv; ++c) {
-    if (threadIdx.x < 32) {
-      double best = -1.0;
-      int bi = c;
-      for (int r = c + threadIdx.x; r < nv; r += 32) {
-        const double v = amag(acc_load(aug[r * w + c]));
-        if (v > best) {
-          best = v;
-          bi = r;
-        }
+}
+
+// Shared (or global) factorization scratch of one system.
+template <typename ET>
+struct FacScratch {
+  ET *aug, *Pi, *Eb, *Lb, *Ub;
+  ET* fcol[2];   // elimination factors, double-buffered across columns
+  int* prow_of;  // pivot row of each column
+  int* used;     // row already pivotal
+  int* ctl;      // [0], [1]: pivot row of the current / next column
+  int nv, w1, nn;
+  __device__ void init(ET* base, int nv_) {
+    nv = nv_;
+    w1 = 2 * nv + 1;
+    nn = nv * nv;
+    aug = base;
+    Pi = aug + nv * w1;
+    Eb = Pi + nn;
+    Lb = Eb + 3 * nn;
+    Ub = Lb + 3 * nn;
+    fcol[0] = Ub + 3 * nn;
+    fcol[1] = fcol[0] + nv;
+    prow_of = reinterpret_cast<int*>(fcol[1] + nv);
+    used = prow_of + nv;
+    ctl = used + nv;
+  }
+};
+
+// Scratch (ET elements) per system for block size nv.
+__host__ __device__ __forceinline__ int blu_smem_elems_v2(int nv) {
+  return nv * (2 * nv + 1) + 10 * nv * nv + 6 * nv + 16;
+}
+
+template <typename ET>
+__device__ void fac_stage(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
+  const int nv = S.nv, nn = S.nn, w1 = S.w1;
+  const ET* P = L.blk(i, 3);
+  for (int e = threadIdx.x; e < nv * 2 * nv; e += blockDim.x) {
+    const int r = e / (2 * nv), c = e - r * (2 * nv);
+    S.aug[r * w1 + c] = c < nv ? P[r * nv + c] : ((c - nv == r) ? fone(ET()) : fzero(ET()));
+  }
+  for (int e = threadIdx.x; e < nr * nn; e += blockDim.x) {
+    const int cc = e / nn, jl = e - cc * nn;
+    S.Ub[e] = L.blk(i, 4 + cc)[jl];
+    S.Eb[e] = L.blk(i + 1 + cc, 2 - cc)[jl];
+  }
+  for (int r = threadIdx.x; r < nv; r += blockDim.x) S.used[r] = 0;
+}
+
+// Pivot selection for column c by warp `wsel` from the column values v[k]
+// (rows lane + 32 k); writes the elimination factors and the pivot row.
+template <typename ET>
+__device__ __forceinline__ bool fac_pick(FacScratch<ET>& S, int c, const ET (&v)[2], int buf) {
+  const int lane = threadIdx.x & 31, nv = S.nv;
+  double best = -1.0;
+  int bi = nv;
+  for (int k = 0; k < 2; ++k) {
+    const int r = lane + 32 * k;
+    if (r < nv && !S.used[r]) {
+      const double m = fmag(v[k]);
+      if (m > best) {
+        best = m;
+        bi = r;
       }
+    }
+  }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) {
-          best = ob;
-          bi = oi;
-        }
-      }
-      if (threadIdx.x == 0) piv_s[0] = bi;
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ob > best || (ob == best && oi < bi)) {
+      best = ob;
+      bi = oi;
     }
-    __syncthreads();
-    const int p = piv_s[0];
-    const A pv = acc_load(aug[p * w + c]);
-    if (amag(pv) == 0.0) ok = false;
-    const A inv = ainv(pv);
-    for (int l = threadIdx.x; l < w; l += blockDim.x) {
-      st_elem(prow[l], amul(acc_load(aug[p * w + l]), inv));
-      orow[l] = aug[c * w + l];
-    }
-    for (int r = threadIdx.x; r < nv; r += blockDim.x) fcol[r] = (r == p) ? aug[c * w + c] : aug[r * w + c];
-    __syncthreads();
-    for (int e = threadIdx.x; e < nv * w; e += blockDim.x) {
-      const int r = e / w, l = e - r * w;
-      if (r == c) {
-        aug[e] = prow[l];
-      } else {
-        const A src = acc_load((r == p) ? orow[l] : aug[e]);
-        st_elem(aug[e], asub(src, amul(acc_load(fcol[r]), acc_load(prow[l]))));
-      }
-    }
-    __syncthreads();
   }
-  for (int e = threadIdx.x; e < nv * nv; e += blockDim.x) {
-    const int r = e / nv, c = e - r * nv;
-    P[e] = aug[r * w + nv + c];
+  const int p = bi < nv ? bi : c;
+  // broadcast the pivot value from its owning lane
+  ET pv;
+  {
+    const int owner = p & 31, kk = p >> 5;
+    ET mine = v[kk < 2 ? kk : 0];
+    if constexpr (IsCx<ET>::v) {
+      pv.re = __shfl_sync(0xffffffffu, mine.re, owner);
+      pv.im = __shfl_sync(0xffffffffu, mine.im, owner);
+    } else {
+      pv = __shfl_sync(0xffffffffu, mine, owner);
+    }
   }
-  __syncthreads();
+  const ET inv = finv(pv);
+  for (int k = 0; k < 2; ++k) {
+    const int r = lane + 32 * k;
+    if (r < nv) S.fcol[buf][r] = (r == p) ? fzero(ET()) : fmul(v[k], inv);
+  }
+  if (lane == 0) {
+    S.ctl[buf] = p;
+    S.used[p] = 1;
+    S.prow_of[c] = p;
+  }
+  return best > 0.0;
+}
+
+// Gauss-Jordan elimination of column c (pivot row ctl[c&1]) by the CTA; warp
+// `wsel` owns column c + 1, updates it first and picks its pivot (look-ahead),
+// so each column costs one barrier.
+template <typename ET>
+__device__ bool fac_elim(FacScratch<ET>& S, int c, int wsel) {
+  const int nv = S.nv, w1 = S.w1, buf = c & 1;
+  const int p = S.ctl[buf];
+  const ET* f = S.fcol[buf];
+  const ET* prow = S.aug + p * w1;
+  bool ok = true;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cn = c + 1;
+  if (warp == wsel && cn < nv) {
+    ET v[2];
+    v[0] = v[1] = fzero(ET());
+    for (int k = 0; k < 2; ++k) {
+      const int r = lane + 32 * k;
+      if (r >= nv) continue;
+      ET& x = S.aug[r * w1 + cn];
+      if (r != p) x = fsub(x, fmul(f[r], prow[cn]));
+      v[k] = x;
+    }
+    ok = fac_pick<ET>(S, cn, v, buf ^ 1);
+  }
+  const int skip = cn < nv ? cn : -1;  // column already updated by the look-ahead warp
+  for (int e = threadIdx.x; e < nv * 2 * nv; e += blockDim.x) {
+    const int r = e / (2 * nv), l = e - r * (2 * nv);
+    if (r == p || l == skip) continue;
+    ET& x = S.aug[r * w1 + l];
+    x = fsub(x, fmul(f[r], prow[l]));
+  }
   return ok;
 }
 
-// Factor in place.  sbig: shared scratch of max(3 nv^2, 2 nv^2 + 6 nv) ET.
 template <typename ET>
-__device__ bool blu_factor(const BlockLU<ET>& L, ET* sbig, int* piv_s) {
-  using A = typename AccOf<ET>::T;
-  const int ns = L.ns, nv = L.nv, nn = nv * nv;
+__device__ void fac_extract(const BlockLU<ET>& L, FacScratch<ET>& S, int i) {
+  const int nv = S.nv, w1 = S.w1;
+  for (int e = threadIdx.x; e < S.nn; e += blockDim.x) {
+    const int c = e / nv, l = e - c * nv;
+    const int p = S.prow_of[c];
+    const ET v = fmul(S.aug[p * w1 + nv + l], finv(S.aug[p * w1 + c]));
+    S.Pi[e] = v;
+    L.blk(i, 3)[e] = v;
+  }
+}
+
+// L_ri = E_ri P^-1 (shared), W_ic = P^-1 U_ic (global)
+template <typename ET>
+__device__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
+  const int nv = S.nv, nn = S.nn, th = (nv + 1) / 2, ntile = th * th;
+  for (int t = threadIdx.x; t < 2 * nr * ntile; t += blockDim.x) {
+    const int job = t / ntile, tt = t - job * ntile;
+    const int j0 = 2 * (tt / th), l0 = 2 * (tt - (tt / th) * th);
+    ET acc[2][2];
+    if (job < nr) {
+      tile2x2<ET>(S.Eb + job * nn, nv, S.Pi, nv, nv, j0, l0, acc);
+      ET* dst = S.Lb + job * nn;
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+          if (j0 + a < nv && l0 + b < nv) dst[(j0 + a) * nv + l0 + b] = acc[a][b];
+    } else {
+      const int cc = job - nr;
+      tile2x2<ET>(S.Pi, nv, S.Ub + cc * nn, nv, nv, j0, l0, acc);
+      ET* W = L.blk(i, 4 + cc);
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+          if (j0 + a < nv && l0 + b < nv) W[(j0 + a) * nv + l0 + b] = acc[a][b];
+    }
+  }
+}
+
+// L blocks out; E_rc -= L_ri U_ic
+template <typename ET>
+__device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
+  const int nv = S.nv, nn = S.nn, th = (nv + 1) / 2, ntile = th * th;
+  for (int e = threadIdx.x; e < nr * nn; e += blockDim.x) {
+    const int rr = e / nn, jl = e - rr * nn;
+    L.blk(i + 1 + rr, 2 - rr)[jl] = S.Lb[e];
+  }
+  for (int t = threadIdx.x; t < nr * nr * ntile; t += blockDim.x) {
+    const int job = t / ntile, tt = t - job * ntile;
+    const int j0 = 2 * (tt / th), l0 = 2 * (tt - (tt / th) * th);
+    const int rr = job / nr, cc = job - rr * nr;
+    ET acc[2][2];
+    tile2x2<ET>(S.Lb + rr * nn, nv, S.Ub + cc * nn, nv, nv, j0, l0, acc);
+    ET* E = L.blk(i + 1 + rr, cc - rr + 3);
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        if (j0 + a < nv && l0 + b < nv) {
+          ET& x = E[(j0 + a) * nv + l0 + b];
+          x = fsub(x, acc[a][b]);
+        }
+  }
+}
+
+// Factor the real stage matrix (and, when LC is given, the complex one in
+// lockstep so both share every barrier).  scr_r / scr_c: scratch of
+// blu_smem_elems_v2(nv) elements each.
+template <typename FT>
+__device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC, FT* scr_r,
+                                Cx<FT>* scr_c) {
+  const int ns = LR.ns, nv = LR.nv;
+  FacScratch<FT> SR;
+  SR.init(scr_r, nv);
+  FacScratch<Cx<FT>> SC;
+  if (LC) SC.init(scr_c, nv);
   bool ok = true;
+  const int warp = threadIdx.x >> 5;
   for (int i = 0; i < ns; ++i) {
-    ET* P = L.blk(i, 3);
-    ok &= gj_invert<ET>(P, nv, sbig, sbig + 2 * nn, piv_s);
     const int nr = min(i + 3, ns - 1) - i;
+    fac_stage<FT>(LR, SR, i, nr);
+    if (LC) fac_stage<Cx<FT>>(*LC, SC, i, nr);
+    __syncthreads();
+    // pivots of column 0 (warp 0: real, warp 1: complex)
+    if (warp == 0) {
+      FT v[2];
+      v[0] = v[1] = fzero(FT());
+      for (int k = 0; k < 2; ++k) {
+        const int r = (threadIdx.x & 31) + 32 * k;
+        if (r < nv) v[k] = SR.aug[r * SR.w1];
+      }
+      ok &= fac_pick<FT>(SR, 0, v, 0);
+    } else if (warp == 1 && LC) {
+      Cx<FT> v[2];
+      v[0] = v[1] = fzero(Cx<FT>());
+      for (int k = 0; k < 2; ++k) {
+        const int r = (threadIdx.x & 31) + 32 * k;
+        if (r < nv) v[k] = SC.aug[r * SC.w1];
+      }
+      ok &= fac_pick<Cx<FT>>(SC, 0, v, 0);
+    }
+    __syncthreads();
+    for (int c = 0; c < nv; ++c) {
+      ok &= fac_elim<FT>(SR, c, 0);
+      if (LC) ok &= fac_elim<Cx<FT>>(SC, c, 1);
+      __syncthreads();
+    }
+    fac_extract<FT>(LR, SR, i);
+    if (LC) fac_extract<Cx<FT>>(*LC, SC, i);
+    __syncthreads();
     if (nr > 0) {
-      // L_ri = E_ri P_i^-1 -> shared
-      for (int e = threadIdx.x; e < nr * nn; e += blockDim.x) {
-        const int rr = e / nn, jl = e - rr * nn, j = jl / nv, l = jl - j * nv;
-        const ET* E = L.blk(i + 1 + rr, 2 - rr);
-        A acc = azero(A());
-        for (int m = 0; m < nv; ++m) afma(acc, acc_load(E[j * nv + m]), acc_load(P[m * nv + l]));
-        st_elem(sbig[e], acc);
-      }
+      fac_lw<FT>(LR, SR, i, nr);
+      if (LC) fac_lw<Cx<FT>>(*LC, SC, i, nr);
       __syncthreads();
-      for (int e = threadIdx.x; e < nr * nn; e += blockDim.x) {
-        const int rr = e / nn, jl = e - rr * nn;
-        L.blk(i + 1 + rr, 2 - rr)[jl] = sbig[e];
-      }
-      // E_rc -= L_ri U_ic for r, c in (i, i + 3]
-      for (int e = threadIdx.x; e < nr * nr * nn; e += blockDim.x) {
-        const int rc2 = e / nn, jl = e - rc2 * nn;
-        const int rr = rc2 / nr, cc = rc2 - rr * nr;
-        const int r = i + 1 + rr, c = i + 1 + cc;
-        const int j = jl / nv, l = jl - j * nv;
-        const ET* Lr = sbig + rr * nn + j * nv;
-        const ET* U = L.blk(i, c - i + 3);
-        A acc = azero(A());
-        for (int m = 0; m < nv; ++m) afma(acc, acc_load(Lr[m]), acc_load(U[m * nv + l]));
-        ET* E = L.blk(r, c - r + 3);
-        st_elem(E[jl], asub(acc_load(E[jl]), acc));
-      }
-      __syncthreads();
-      // W_ik = P_i^-1 U_ik (in place via shared staging)
-      for (int e = threadIdx.x; e < nr * nn; e += blockDim.x) {
-        const int cc = e / nn, jl = e - cc * nn, j = jl / nv, l = jl - j * nv;
-        const ET* U = L.blk(i, 4 + cc);
-        A acc = azero(A());
-        for (int m = 0; m < nv; ++m) afma(acc, acc_load(P[j * nv + m]), acc_load(U[m * nv + l]));
-        st_elem(sbig[e], acc);
-      }
-      __syncthreads();
-      for (int e = threadIdx.x; e < nr * nn; e += blockDim.x) {
-        const int cc = e / nn, jl = e - cc * nn;
-        L.blk(i, 4 + cc)[jl] = sbig[e];
-      }
+      fac_update<FT>(LR, SR, i, nr);
+      if (LC) fac_update<Cx<FT>>(*LC, SC, i, nr);
       __syncthreads();
     }
   }

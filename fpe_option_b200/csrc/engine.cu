@@ -62,6 +62,8 @@ Context& ctx() {
     }
     int lim = c.smem_optin;
     if (cudaFuncSetAttribute(fpe::k_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess) return;
+    const int ic_lim = lim - int(sizeof(fpe::IcSmem)) - 1024;
+    if (cudaFuncSetAttribute(fpe::k_ic, cudaFuncAttributeMaxDynamicSharedMemorySize, ic_lim) != cudaSuccess) return;
     if (cudaFuncSetAttribute(fpe::k_radau<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess) return;
     if (cudaFuncSetAttribute(fpe::k_radau<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess) return;
     c.ok = true;
@@ -217,6 +219,8 @@ struct FpePlan {
   double* d_traj = nullptr;
   int64_t n_d = 0, n_i = 0, n_f = 0, n_traj = 0;
   size_t radau_smem = 0, setup_smem = 0;
+  int fac_global = 0;
+  size_t ic_smem = 0;
   int n_price_slots = 0;
   // host results
   std::vector<double> h_prices;
@@ -227,7 +231,7 @@ struct FpePlan {
 
 static int plan_layout(FpePlan* P, int esz) {
   int64_t od = 0, oi = 0, of = 0, ot = 0;
-  size_t smem_max = 0;
+  size_t smem_max = 0, smem_base_max = 0;
   const int cplx = P->o.complex_mode;
   for (auto& d : P->descs) {
     d.off_d = od;
@@ -243,15 +247,30 @@ static int plan_layout(FpePlan* P, int esz) {
     const int nv = std::min(d.cap_dof_v, FPE_MAX_NDOF_V);
     const int ns_cap = std::min(d.cap_dof_s, FPE_MAX_NDOF_S);
     const int ebytes = cplx ? 2 * esz : esz;  // the complex factor needs the larger scratch
-    size_t sm = sizeof(fpe::RadauSmem) + size_t(4 * ns_cap * 7 + 5 * nv * 7) * 8 +
-                size_t(std::max(3 * nv * nv, 2 * nv * nv + 6 * nv)) * ebytes + 64;
+    size_t base = sizeof(fpe::RadauSmem) + size_t(4 * ns_cap * 7 + 5 * nv * 7) * 8 + 64;
+    size_t sm = base + size_t(fpe::blu_smem_elems_v2(nv)) * esz +
+                (cplx ? size_t(fpe::blu_smem_elems_v2(nv)) * 2 * esz + 16 : 0);
+    (void)ebytes;
+    smem_base_max = std::max(smem_base_max, base);
     smem_max = std::max(smem_max, sm);
   }
   P->n_d = od;
   P->n_i = oi;
   P->n_f = of;
   P->n_traj = ot;
-  P->radau_smem = smem_max;
+  // stage the factorization in shared memory when it fits the opt-in limit,
+  // otherwise keep its scratch in the solve's global work area
+  const size_t optin = size_t(ctx().smem_optin > 0 ? ctx().smem_optin : 232448);
+  P->fac_global = smem_max > optin ? 1 : 0;
+  // ADMM iterates of the IC projection in shared memory when they fit
+  size_t ic = 0;
+  for (auto& d : P->descs) {
+    const size_t ns = d.cap_dof_s, nv = d.cap_dof_v;
+    ic = std::max(ic, (ns * ns + nv * nv + 7 * ns * nv) * sizeof(double));
+  }
+  const size_t ic_lim = optin - sizeof(fpe::IcSmem) - 1024;
+  P->ic_smem = ic <= ic_lim ? ic : 0;
+  P->radau_smem = P->fac_global ? smem_base_max : smem_max;
   P->setup_smem = sizeof(fpe::SetupSmem);
   return 0;
 }
@@ -291,18 +310,21 @@ static int plan_launch(FpePlan* P, cudaStream_t s, int from, int to) {
     ++launches;
   }
   if (from <= 2 && to > 2) {
-    fpe::k_ic<<<grid, block, 0, s>>>(P->d_descs, P->d_arena, P->d_iarena, P->d_infos);
+    fpe::k_ic<<<grid, block, P->ic_smem, s>>>(P->d_descs, P->d_arena, P->d_iarena, P->d_infos,
+                                              P->ic_smem);
     ++launches;
   }
   if (from <= 3 && to > 3) {
     const fpe::RadauConstants rk = fpe::radau_constants(P->o.radau_exact != 0);
     if (P->o.precision == 0) {
       fpe::RadauKernelArgs<double> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena,
-                                     P->d_traj, 0, P->o.complex_mode, rk.u1, rk.alph, rk.beta, rk.ti13};
+                                     P->d_traj, 0, P->o.complex_mode, P->fac_global,
+                                     rk.u1, rk.alph, rk.beta, rk.ti13};
       fpe::k_radau<double><<<grid, block, P->radau_smem, s>>>(a);
     } else {
       fpe::RadauKernelArgs<float> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena,
-                                    P->d_traj, P->o.refine, P->o.complex_mode, rk.u1, rk.alph, rk.beta, rk.ti13};
+                                    P->d_traj, P->o.refine, P->o.complex_mode, P->fac_global,
+                                    rk.u1, rk.alph, rk.beta, rk.ti13};
       fpe::k_radau<float><<<grid, block, P->radau_smem, s>>>(a);
     }
     ++launches;
@@ -690,7 +712,7 @@ int32_t fpe_plan_results(FpePlan* P, double* prices, double* delta, double* gamm
 int32_t fpe_plan_stats(FpePlan* P, int64_t* out) {
   if (!P || !out) return -1;
   if (plan_fetch(P) < 0) return -1;
-  for (int k = 0; k < 16; ++k) out[k] = 0;
+  for (int k = 0; k < 20; ++k) out[k] = 0;
   out[0] = int64_t(P->descs.size());
   for (size_t s = 0; s < P->descs.size(); ++s) {
     const int32_t* in = &P->h_infos[s * FPE_INFO_COUNT];
@@ -713,6 +735,10 @@ int32_t fpe_plan_stats(FpePlan* P, int64_t* out) {
     out[12] += int64_t(in[FPE_INFO_PASS_REAL]) * R + int64_t(in[FPE_INFO_PASS_CPLX]) * Cb +
                int64_t(in[FPE_INFO_LU]) * (R + Cb);
     out[13] = std::max<int64_t>(out[13], in[FPE_INFO_STATUS]);
+    out[14] += in[FPE_INFO_T_FACTOR];
+    out[15] += in[FPE_INFO_T_SOLVE];
+    out[16] += in[FPE_INFO_T_KRON];
+    out[17] += in[FPE_INFO_T_TOTAL];
   }
   return 0;
 }

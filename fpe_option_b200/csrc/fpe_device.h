@@ -30,7 +30,9 @@ enum FpeInfo {
   FPE_INFO_NQ_S, FPE_INFO_NQ_V, FPE_INFO_NDOF_S, FPE_INFO_NDOF_V,
   FPE_INFO_ACCEPTED, FPE_INFO_REJECTED, FPE_INFO_NEWTON, FPE_INFO_GMRES, FPE_INFO_LU,
   FPE_INFO_ADMM, FPE_INFO_PASS_REAL, FPE_INFO_NSAVED, FPE_INFO_PASS_CPLX,
-  FPE_INFO_COUNT = 20
+  // SM clock cycles / 1024 spent in the Radau kernel phases (thread 0's view)
+  FPE_INFO_T_FACTOR, FPE_INFO_T_SOLVE, FPE_INFO_T_KRON, FPE_INFO_T_TOTAL,
+  FPE_INFO_COUNT = 24
 };
 
 struct FpeSolveDesc {
@@ -68,6 +70,7 @@ struct FpeDLayout {
   int64_t fac_s, fac_v;                             // raw 1-D Galerkin factors
   int64_t op_s, op_v, D_s, D_v, m_s, m_v;           // scaled operator factors
   int64_t proj, q0, y, qT;                          // vectors of length N
+  int64_t fsc;                                      // factorization scratch (global fallback)
   int64_t work;                                     // Radau/GMRES/ADMM work area
   int64_t total;
 };
@@ -129,6 +132,9 @@ FPE_HD FpeDLayout fpe_dlayout(const FpeSolveDesc& d) {
   L.q0 = take(N);
   L.y = take(N);
   L.qT = take(N);
+  // FP64 worst case of the real + complex factor scratch:
+  // 3 x (nv (2nv+1) + 10 nv^2 + 6 nv + 16) doubles + alignment
+  L.fsc = take(40 * int64_t(d.cap_dof_v) * d.cap_dof_v + 64 * int64_t(d.cap_dof_v) + 128);
   int64_t dense = int64_t(d.cap_dof_s) * d.cap_dof_s + int64_t(d.cap_dof_v) * d.cap_dof_v;
   L.work = take(int64_t(FPE_WORK_VECS) * N + 4 * dense + 256);
   L.total = o;

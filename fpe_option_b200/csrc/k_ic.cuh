@@ -28,6 +28,30 @@ __device__ void cta_gemm(int m, int n, int k, const double* __restrict__ A, int 
   }
 }
 
+// Same product with two adjacent outputs per thread (shared-memory operands);
+// when scale is given the result is multiplied elementwise by it.
+__device__ void cta_gemm2(int m, int n, int k, const double* __restrict__ A, int ar, int ac,
+                          const double* __restrict__ B, int br, int bc, double* __restrict__ C,
+                          int ldc, const double* __restrict__ scale) {
+  const int n2 = (n + 1) / 2;
+  for (int e = threadIdx.x; e < m * n2; e += blockDim.x) {
+    const int r = e / n2, c = 2 * (e - r * n2);
+    const int c1 = c + 1 < n ? c + 1 : c;
+    double a0 = 0.0, a1 = 0.0;
+    for (int p = 0; p < k; ++p) {
+      const double av = A[r * ar + p * ac];
+      a0 = fma(av, B[p * br + c * bc], a0);
+      a1 = fma(av, B[p * br + c1 * bc], a1);
+    }
+    if (scale) {
+      a0 *= scale[r * ldc + c];
+      a1 *= scale[r * ldc + c1];
+    }
+    C[r * ldc + c] = a0;
+    if (c + 1 < n) C[r * ldc + c + 1] = a1;
+  }
+}
+
 // Cyclic Jacobi eigendecomposition of the symmetric n x n matrix A (row-major,
 // destroyed; eigenvalues left on its diagonal), eigenvectors in the columns
 // of V.  Round-robin ordering: n/2 disjoint rotations per round.
@@ -167,8 +191,10 @@ struct IcSmem {
 
 __global__ void __launch_bounds__(FPE_BLOCK) k_ic(const FpeSolveDesc* __restrict__ descs,
                                                   double* __restrict__ darena,
-                                                  int32_t* __restrict__ iarena, int32_t* __restrict__ infos) {
+                                                  int32_t* __restrict__ iarena, int32_t* __restrict__ infos,
+                                                  size_t dyn_bytes) {
   __shared__ IcSmem S;
+  extern __shared__ __align__(16) unsigned char ic_dyn[];
   const FpeSolveDesc d = descs[blockIdx.x];
   const FpeDLayout DL = fpe_dlayout(d);
   const FpeILayout IL = fpe_ilayout(d);
@@ -312,30 +338,56 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_ic(const FpeSolveDesc* __restrict
   __syncthreads();
 
   // ---- ADMM (osqp.mojo:93-157) ------------------------------------------
+  // Shared-memory resident when it fits (eigenvectors + five iterates + lam, q).
+  const size_t need = (size_t(nds) * nds + size_t(ndv) * ndv + 7 * size_t(N)) * sizeof(double);
+  double* sVs = Vs;
+  double* sVv = Vv;
+  double *sx = x, *sz = z, *su = u, *sq = q, *srhs = rhs, *st1 = t1, *slam = lam;
+  if (need <= dyn_bytes) {
+    double* sm = reinterpret_cast<double*>(ic_dyn);
+    sVs = sm;
+    sVv = sVs + nds * nds;
+    sx = sVv + ndv * ndv;
+    sz = sx + N;
+    su = sz + N;
+    sq = su + N;
+    srhs = sq + N;
+    st1 = srhs + N;
+    slam = st1 + N;
+    for (int e = threadIdx.x; e < nds * nds; e += blockDim.x) sVs[e] = Vs[e];
+    for (int e = threadIdx.x; e < ndv * ndv; e += blockDim.x) sVv[e] = Vv[e];
+    for (int e = threadIdx.x; e < N; e += blockDim.x) {
+      sx[e] = 0.0;
+      sz[e] = 0.0;
+      su[e] = 0.0;
+      sq[e] = q[e];
+      slam[e] = lam[e];
+    }
+    __syncthreads();
+  }
   int it = 0;
   for (it = 0; it < 50000; ++it) {
-    for (int e = threadIdx.x; e < N; e += blockDim.x) rhs[e] = q[e] + rho * (z[e] - u[e]) + sigma * x[e];
+    for (int e = threadIdx.x; e < N; e += blockDim.x)
+      srhs[e] = sq[e] + rho * (sz[e] - su[e]) + sigma * sx[e];
     __syncthreads();
     // x = (Vs (x) Vv) diag(lam) (Vs (x) Vv)^T rhs
-    cta_gemm(nds, ndv, nds, Vs, 1, nds, rhs, ndv, 1, t1, ndv);  // Vs^T R
+    cta_gemm2(nds, ndv, nds, sVs, 1, nds, srhs, ndv, 1, st1, ndv, nullptr);  // Vs^T R
     __syncthreads();
-    cta_gemm(nds, ndv, ndv, t1, ndv, 1, Vv, ndv, 1, x, ndv);  // (Vs^T R) Vv
+    cta_gemm2(nds, ndv, ndv, st1, ndv, 1, sVv, ndv, 1, sx, ndv, slam);  // ((Vs^T R) Vv) .* lam
     __syncthreads();
-    for (int e = threadIdx.x; e < N; e += blockDim.x) x[e] *= lam[e];
+    cta_gemm2(nds, ndv, nds, sVs, nds, 1, sx, ndv, 1, st1, ndv, nullptr);  // Vs X
     __syncthreads();
-    cta_gemm(nds, ndv, nds, Vs, nds, 1, x, ndv, 1, t1, ndv);  // Vs X
-    __syncthreads();
-    cta_gemm(nds, ndv, ndv, t1, ndv, 1, Vv, 1, ndv, x, ndv);  // (Vs X) Vv^T
+    cta_gemm2(nds, ndv, ndv, st1, ndv, 1, sVv, 1, ndv, sx, ndv, nullptr);  // (Vs X) Vv^T
     __syncthreads();
     double nr[5] = {0, 0, 0, 0, 0};
     for (int e = threadIdx.x; e < N; e += blockDim.x) {
-      const double xe = x[e];
-      double zn = xe + u[e];
+      const double xe = sx[e];
+      double zn = xe + su[e];
       if (zn < 0.0) zn = 0.0;
-      const double zo = z[e];
-      z[e] = zn;
-      const double un = u[e] + xe - zn;
-      u[e] = un;
+      const double zo = sz[e];
+      sz[e] = zn;
+      const double un = su[e] + xe - zn;
+      su[e] = un;
       const double pv = xe - zn, dv = rho * (zn - zo);
       nr[0] += pv * pv;
       nr[1] += dv * dv;
@@ -350,6 +402,10 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_ic(const FpeSolveDesc* __restrict
       ++it;
       break;
     }
+  }
+  if (sz != z) {
+    for (int e = threadIdx.x; e < N; e += blockDim.x) z[e] = sz[e];
+    __syncthreads();
   }
   // ---- q0 = max(Dinv c, 0) normalised by m^T q0 ---------------------------
   double* q0 = D + DL.q0;

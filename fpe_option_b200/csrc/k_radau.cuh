@@ -122,6 +122,7 @@ struct RadauKernelArgs {
   double* traj;
   int nref;          // extra FP64 refinement sweeps per stage solve
   int complex_mode;  // 0 GMRES(10) with E1 preconditioner, 1 complex block LU
+  int fac_global;    // factorization scratch in global memory (too large for shared)
   // Eigenvalues of the Radau IIA A^-1 (gamma, alpha +- i beta) and TI13 of the
   // transformation.  The reference hard-codes U1 = 3.6378165692476072,
   // ALPH = 2.6753213032678365, BETA = 3.0493570545593676 and
@@ -173,7 +174,11 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
   // shared memory: RadauSmem | fs (4 ns 7) | fv (5 nv 7) | factor scratch
   double* fs = reinterpret_cast<double*>(smem_raw + sizeof(RadauSmem));
   double* fv = fs + 4 * ns * 7;
-  void* sbig = reinterpret_cast<void*>(fv + 5 * nv * 7);
+  // factor scratch, 16-byte aligned (complex FP64 elements)
+  void* sbig = A.fac_global
+                   ? reinterpret_cast<void*>(D + DL.fsc)
+                   : reinterpret_cast<void*>((reinterpret_cast<uintptr_t>(fv + 5 * nv * 7) + 15) &
+                                             ~uintptr_t(15));
   for (int e = threadIdx.x; e < 4 * ns * 7; e += blockDim.x) fs[e] = D[DL.op_s + e];
   for (int e = threadIdx.x; e < 5 * nv * 7; e += blockDim.x) fv[e] = D[DL.op_v + e];
   __syncthreads();
@@ -204,9 +209,19 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
   const double* Dsv = D + DL.D_s;
   const double* Dvv = D + DL.D_v;
 
+  // phase timers (SM clock cycles, thread 0 reports)
+  const long long t_kernel0 = clock64();
+  long long t_factor = 0, t_solve = 0, t_kron = 0;
+#define KRON(...)                          \
+  do {                                     \
+    const long long t_k0 = clock64();      \
+    kron_apply(__VA_ARGS__);               \
+    t_kron += clock64() - t_k0;            \
+  } while (0)
   // block solves ------------------------------------------------------------
   long n_pass_r = 0, n_pass_c = 0;  // sweeps over the real / complex factors
   auto solve_set = [&](double* xr0, double* xr1, int nr, double* xc_re, double* xc_im, int nc) {
+    const long long t_s0 = clock64();
     n_pass_r += nr > 0;
     n_pass_c += nc > 0;
     SolveSet<FT> Sv;
@@ -223,6 +238,7 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
     Sv.zc_im = vslot(C, RV_ZC);
     Sv.nc = nc;
     blu_solve<FT>(Sv);
+    t_solve += clock64() - t_s0;
   };
   KronTerm E1t[5], Edt[5];
   // x = E1^-1 b (+ nref FP64 refinement sweeps)
@@ -294,12 +310,14 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
       need_lu = hr < quot1 || hr > quot2;
     }
     if (need_lu) {
+      const long long t_f0 = clock64();
       blu_assemble<FT>(O, LR, U1, 0.0, h);
-      if (!blu_factor<FT>(LR, reinterpret_cast<FT*>(sbig), S.piv)) status = FPE_ERR_SINGULAR;
-      if (direct) {
-        blu_assemble<Cx<FT>>(O, LC, ALPH, BETA, h);
-        if (!blu_factor<Cx<FT>>(LC, reinterpret_cast<Cx<FT>*>(sbig), S.piv)) status = FPE_ERR_SINGULAR;
-      }
+      if (direct) blu_assemble<Cx<FT>>(O, LC, ALPH, BETA, h);
+      FT* scr_r = reinterpret_cast<FT*>(sbig);
+      Cx<FT>* scr_c = reinterpret_cast<Cx<FT>*>(
+          (reinterpret_cast<uintptr_t>(scr_r + blu_smem_elems_v2(nv)) + 15) & ~uintptr_t(15));
+      if (!blu_factor_pair<FT>(LR, direct ? &LC : nullptr, scr_r, scr_c)) status = FPE_ERR_SINGULAR;
+      t_factor += clock64() - t_f0;
       ++n_lu;
       h_lu = h;
       E1t[0] = {O.As, O.Av, U1};
@@ -313,7 +331,7 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
     {
       const double* xi[1] = {y};
       double* yo[1] = {w};
-      kron_apply(C, Kt, 4, xi, yo, 1);
+      KRON(C, Kt, 4, xi, yo, 1);
     }
     if (first || reject) {
       for (int e = threadIdx.x; e < N; e += blockDim.x) {
@@ -345,10 +363,10 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
       {
         const double* xi[3] = {Z1, Z2, Z3};
         double* yo[3] = {KZ1, KZ2, KZ3};
-        kron_apply(C, Kt, 4, xi, yo, 3);
+        KRON(C, Kt, 4, xi, yo, 3);
         const double* xm[3] = {F1, F2, F3};
         double* ym[3] = {MF1, MF2, MF3};
-        kron_apply(C, Mt, 1, xm, ym, 3);
+        KRON(C, Mt, 1, xm, ym, 3);
       }
       for (int e = threadIdx.x; e < N; e += blockDim.x) {  // radau.mojo:575-630
         const double f1 = -w[e] - KZ1[e], f2 = -w[e] - KZ2[e], f3 = -w[e] - KZ3[e];
@@ -372,7 +390,7 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
         for (int it = 0; it < A.nref; ++it) {
           const double* xc[1] = {dF1};
           double* rs[1] = {res};
-          kron_apply(C, E1t, 5, xc, rs, 1);
+          KRON(C, E1t, 5, xc, rs, 1);
           apply_E2(C, Edt, Mt, BETA, dF2, dF3, res2, res3, wr, wi);
           for (int e = threadIdx.x; e < N; e += blockDim.x) {
             res[e] = rr[e] - res[e];
@@ -572,7 +590,7 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
     {
       const double* xm[1] = {CERR};
       double* ym[1] = {MCONT};
-      kron_apply(C, Mt, 1, xm, ym, 1);
+      KRON(C, Mt, 1, xm, ym, 1);
     }
     for (int e = threadIdx.x; e < N; e += blockDim.x) rerr[e] = MCONT[e] - h * w[e];
     __syncthreads();
@@ -590,7 +608,7 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
       {
         const double* xi[1] = {yt};
         double* yo[1] = {w};
-        kron_apply(C, Kt, 4, xi, yo, 1);
+        KRON(C, Kt, 4, xi, yo, 1);
       }
       for (int e = threadIdx.x; e < N; e += blockDim.x) rerr[e] = MCONT[e] - h * w[e];
       __syncthreads();
@@ -654,6 +672,10 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
     info[FPE_INFO_NSAVED] = n_saved;
     info[FPE_INFO_PASS_REAL] = int(n_pass_r);
     info[FPE_INFO_PASS_CPLX] = int(n_pass_c);
+    info[FPE_INFO_T_FACTOR] = int(t_factor >> 10);
+    info[FPE_INFO_T_SOLVE] = int(t_solve >> 10);
+    info[FPE_INFO_T_KRON] = int(t_kron >> 10);
+    info[FPE_INFO_T_TOTAL] = int((clock64() - t_kernel0) >> 10);
   }
 }
 

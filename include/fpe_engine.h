@@ -192,12 +192,13 @@ extern int32_t fpe_plan_run(FpePlan* plan, void* cuda_stream);
  *  every solve succeeded, otherwise the first non-zero status. */
 extern int32_t fpe_plan_results(FpePlan* plan, double* prices, double* delta, double* gamma,
                                 double* vega, int32_t* status);
-/** Aggregated solver counters (16 slots): out[0] solves, [1] accepted steps,
+/** Aggregated solver counters (20 slots): out[0] solves, [1] accepted steps,
  *  [2] rejected, [3] Newton iterations, [4] GMRES iterations, [5] LU
  *  factorizations, [6] ADMM iterations, [7] max n_dof_s, [8] max n_dof_v,
  *  [9] total dofs, [10] sweeps over real factors, [11] sweeps over complex
  *  factors, [12] algorithmic stage-factor bytes (written + read), [13] worst
- *  status. */
+ *  status, [14]-[17] SM kilo-cycles summed over solves spent in the Radau
+ *  kernel's factorizations, block solves, Kronecker products and in total. */
 extern int32_t fpe_plan_stats(FpePlan* plan, int64_t* out);
 /** Run the pipeline once with a CUDA event around each of its five kernels
  *  (setup, galerkin, ic, radau, payoff); ms[5] receives the durations. */
