@@ -65,7 +65,7 @@ EXPORTED = [
     "fpe_compute_free_oneshot", "fpe_plan_create", "fpe_plan_run", "fpe_plan_results",
     "fpe_plan_stats", "fpe_plan_sizes", "fpe_plan_destroy", "fpe_price_batch",
     "fpe_compute_create_ex", "fpe_compute_basis_csr", "fpe_device_available",
-    "fpe_plan_kernel_times",
+    "fpe_plan_kernel_times", "fpe_price_noalloc",
 ]
 
 _lib = None
@@ -122,5 +122,7 @@ def load():
     L.fpe_compute_basis_csr.argtypes = [cp, i32, ip, ip, ip, ip, dp]
     L.fpe_device_available.restype = i32
     L.fpe_device_available.argtypes = []
+    L.fpe_price_noalloc.restype = i32
+    L.fpe_price_noalloc.argtypes = [C.POINTER(FpeContract), C.POINTER(FpeBatchOptions), dp, ip, vp]
     _lib = L
     return L

@@ -1010,3 +1010,195 @@ void fpe_compute_free_oneshot(FpeOneshotResult* r) {
 }
 
 }  // extern "C"
+
+// ==========================================================================
+// Allocation-free pricing of one contract.
+//
+// Some callers cannot allocate device memory at pricing time: code that runs
+// while a CUDA stream is being captured into a graph (allocation calls there
+// either fail or get frozen into the graph), real-time and embedded hosts whose
+// GPU memory budget is fixed at start-up, and plug-ins living inside another
+// application that owns the device memory pool.  fpe_price_noalloc serves them
+// from one file-scope static device array instead of per-call allocations; the
+// caller passes the contract and receives the prices.
+//
+// The array (FPE_NOALLOC_SCRATCH_BYTES, 64 MiB) is held by every GPU that loads
+// this library until the process exits.  Its device address is obtained with
+// cudaGetSymbolAddress once per device, on that device's first call (so make
+// the first call on each device before any stream capture).  Every call shares
+// the array and it keeps the previous call's contents: the per-solve status
+// words and the price slots are cleared at the start of each call, everything
+// else is fully rewritten by the kernels.  Calls that overlap on the GPU (the
+// same device, different streams or threads without ordering) race on the
+// array and must be serialized by the caller.
+// ==========================================================================
+#define FPE_NOALLOC_SCRATCH_BYTES (64ull << 20)
+#define FPE_NOALLOC_MAX_DEVICES 64
+static __device__ __align__(256) unsigned char g_fpe_noalloc_scratch[FPE_NOALLOC_SCRATCH_BYTES];
+
+static unsigned char* noalloc_base(int device, int* err) {
+  static unsigned char* base[FPE_NOALLOC_MAX_DEVICES] = {nullptr};
+  static std::mutex mu;
+  if (device < 0 || device >= FPE_NOALLOC_MAX_DEVICES) {
+    *err = -1;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!base[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_fpe_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      *err = -1;
+      return nullptr;
+    }
+    base[device] = static_cast<unsigned char*>(p);
+  }
+  return base[device];
+}
+
+extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatchOptions* opt,
+                                     double* prices, int32_t* status, void* cuda_stream) {
+  if (!contract || !prices) return -1;
+  const int nk = contract->n_strikes;
+  if (nk <= 0 || nk > FPE_MAX_STRIKES || !contract->strikes) return FPE_NOALLOC_ERR_SIZE;
+  if (opt && opt->greeks) return -1;
+  Context& C = ctx();
+  if (!C.ok) return -1;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  int err = 0;
+  unsigned char* base = noalloc_base(dev, &err);
+  if (!base) return -1;
+  cudaStream_t s = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : C.stream;
+  const Opts o = opts_from(opt, 50);
+
+  // Pricing and its one or two device solves (in-out parity for knock-ins).
+  Pricing p;
+  p.kappa = contract->kappa; p.theta = contract->theta; p.sigma = contract->sigma;
+  p.rho = contract->rho; p.r = contract->r; p.T = contract->T; p.S0 = contract->S0;
+  p.V0 = contract->V0; p.barrier = contract->barrier;
+  p.smin = contract->s_min >= 0.0 ? contract->s_min : 0.0;
+  p.smax = contract->s_max > 0.0 ? contract->s_max : contract->S0 * 3.0;
+  p.n_s = contract->n_s; p.n_v = contract->n_v; p.type = contract->option_type;
+  p.strike_begin = 0;
+  p.n_strikes = nk;
+  p.valid = pricing_valid(p, contract->strikes) && p.n_s >= 4 && p.n_v >= 4 && p.n_s <= 256 &&
+            p.n_v <= 256 && !(o.disc == 0 && grid_count_reference(o.num_insert, true) > 8192);
+  if (!p.valid) {
+    for (int j = 0; j < nk; ++j) {
+      prices[j] = 0.0;
+      if (status) status[j] = FPE_STATUS_INVALID;
+    }
+    return FPE_STATUS_INVALID;
+  }
+  FpeSolveDesc d[2];
+  int nsolve = 1;
+  const int ot = p.type;
+  if (ot == 0 || ot == 1 || ot == 4 || ot == 5) {
+    const bool call = ot % 2 == 0, down = ot <= 1;
+    d[0] = make_desc(p, call ? 8 : 9, 0.0, o);
+    d[1] = make_desc(p, (down ? 2 : 6) + (call ? 0 : 1), p.barrier, o);
+    nsolve = 2;
+  } else {
+    d[0] = make_desc(p, ot, p.barrier, o);
+  }
+
+  // Partition the static array: descriptors | strikes | prices | infos | arenas.
+  const int esz = o.precision == 0 ? 8 : 4;
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  size_t off = 0;
+  const size_t off_desc = off;
+  off = up(off + 2 * sizeof(FpeSolveDesc));
+  const size_t off_k = off;
+  off = up(off + size_t(2) * nk * sizeof(double));
+  const size_t off_p = off;
+  off = up(off + size_t(2) * nk * sizeof(double));
+  const size_t off_info = off;
+  off = up(off + size_t(2) * FPE_INFO_COUNT * sizeof(int32_t));
+  int64_t od = 0, oi = 0, of = 0;
+  size_t smem_max = 0, smem_base = 0, ic = 0;
+  for (int k = 0; k < nsolve; ++k) {
+    d[k].strike_off = k * nk;
+    d[k].off_d = od;
+    d[k].off_i = oi;
+    d[k].off_f = of;
+    d[k].save_traj = 0;
+    d[k].traj_cap = 0;
+    d[k].off_traj = -1;
+    od += fpe_dlayout(d[k]).total;
+    oi += fpe_ilayout(d[k]).total;
+    of += fpe_factor_bytes(d[k], esz, o.complex_mode);
+    const int nv = std::min(d[k].cap_dof_v, FPE_MAX_NDOF_V);
+    const int ns_cap = std::min(d[k].cap_dof_s, FPE_MAX_NDOF_S);
+    const size_t b = sizeof(fpe::RadauSmem) + size_t(4 * ns_cap * 7 + 5 * nv * 7) * 8 + 64;
+    smem_base = std::max(smem_base, b);
+    smem_max = std::max(smem_max, b + size_t(fpe::blu_smem_elems_v2(nv)) * esz +
+                                      (o.complex_mode ? size_t(fpe::blu_smem_elems_v2(nv)) * 2 * esz + 16 : 0));
+    const size_t nsd = d[k].cap_dof_s, nvd = d[k].cap_dof_v;
+    ic = std::max(ic, (nsd * nsd + nvd * nvd + 7 * nsd * nvd) * sizeof(double));
+  }
+  const size_t off_d = off;
+  off = up(off + size_t(od) * sizeof(double));
+  const size_t off_i = off;
+  off = up(off + size_t(oi) * sizeof(int32_t));
+  const size_t off_f = off;
+  off = up(off + size_t(of));
+  if (off > FPE_NOALLOC_SCRATCH_BYTES) {
+    for (int j = 0; j < nk; ++j) {
+      prices[j] = 0.0;
+      if (status) status[j] = FPE_STATUS_CAPACITY;
+    }
+    return FPE_NOALLOC_ERR_SIZE;  // the contract's grids need more than the static array
+  }
+  const size_t optin = size_t(C.smem_optin > 0 ? C.smem_optin : 232448);
+  const int fac_global = smem_max > optin ? 1 : 0;
+  const size_t radau_smem = fac_global ? smem_base : smem_max;
+  const size_t ic_smem = ic <= optin - sizeof(fpe::IcSmem) - 1024 ? ic : 0;
+
+  auto* g_desc = reinterpret_cast<FpeSolveDesc*>(base + off_desc);
+  auto* g_k = reinterpret_cast<double*>(base + off_k);
+  auto* g_p = reinterpret_cast<double*>(base + off_p);
+  auto* g_info = reinterpret_cast<int32_t*>(base + off_info);
+  auto* g_d = reinterpret_cast<double*>(base + off_d);
+  auto* g_i = reinterpret_cast<int32_t*>(base + off_i);
+  auto* g_f = reinterpret_cast<unsigned char*>(base + off_f);
+  CK(cudaMemcpyAsync(g_desc, d, nsolve * sizeof(FpeSolveDesc), cudaMemcpyHostToDevice, s));
+  for (int k = 0; k < nsolve; ++k)
+    CK(cudaMemcpyAsync(g_k + k * nk, contract->strikes, nk * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(g_p, 0, size_t(2) * nk * sizeof(double), s));
+  CK(cudaMemsetAsync(g_info, 0, size_t(2) * FPE_INFO_COUNT * sizeof(int32_t), s));
+  const dim3 grid(nsolve), block(FPE_BLOCK);
+  fpe::k_setup<<<grid, block, sizeof(fpe::SetupSmem), s>>>(g_desc, g_d, g_i, g_info);
+  fpe::k_galerkin<<<grid, block, 0, s>>>(g_desc, g_d, g_i, g_info);
+  fpe::k_ic<<<grid, block, ic_smem, s>>>(g_desc, g_d, g_i, g_info, ic_smem);
+  const fpe::RadauConstants rk = fpe::radau_constants(o.radau_exact != 0);
+  if (o.precision == 0) {
+    fpe::RadauKernelArgs<double> a{g_desc, g_d, g_i, g_info, g_f, nullptr, 0, o.complex_mode,
+                                   fac_global, rk.u1, rk.alph, rk.beta, rk.ti13};
+    fpe::k_radau<double><<<grid, block, radau_smem, s>>>(a);
+  } else {
+    fpe::RadauKernelArgs<float> a{g_desc, g_d, g_i, g_info, g_f, nullptr, o.refine, o.complex_mode,
+                                  fac_global, rk.u1, rk.alph, rk.beta, rk.ti13};
+    fpe::k_radau<float><<<grid, block, radau_smem, s>>>(a);
+  }
+  fpe::k_payoff<<<grid, block, 0, s>>>(g_desc, g_d, g_i, g_info, g_k, g_p);
+  CK(cudaGetLastError());
+  double hp[2 * FPE_MAX_STRIKES];
+  int32_t hi[2 * FPE_INFO_COUNT];
+  CK(cudaMemcpyAsync(hp, g_p, size_t(nsolve) * nk * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hi, g_info, size_t(nsolve) * FPE_INFO_COUNT * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  int worst = 0;
+  for (int j = 0; j < nk; ++j) {
+    double v = hp[j];
+    int st = hi[FPE_INFO_STATUS];
+    if (nsolve == 2) {
+      v -= hp[nk + j];
+      if (!st) st = hi[FPE_INFO_COUNT + FPE_INFO_STATUS];
+    }
+    prices[j] = v;
+    if (status) status[j] = st;
+    if (st && !worst) worst = st;
+  }
+  return worst;
+}

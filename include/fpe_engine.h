@@ -229,6 +229,28 @@ extern int64_t fpe_compute_basis_csr(FpeCompute* ptr, int32_t which, int32_t* n_
 /** Device availability: 1 when a CUDA device can run the kernels. */
 extern int32_t fpe_device_available(void);
 
+/** Returned by fpe_price_noalloc when a contract's grids need more scratch than
+ *  its static array holds (or n_strikes is outside 1..1024). */
+#define FPE_NOALLOC_ERR_SIZE (-2)
+
+/** Price one contract without allocating any memory.
+ *
+ *  No counterpart in the reference (which allocates per call).  For callers
+ *  that cannot allocate device memory while pricing: code running during CUDA
+ *  stream capture, hosts whose GPU memory budget is fixed at start-up, and
+ *  plug-ins inside an application that owns the device memory pool.  All
+ *  device scratch comes from one static device array of 64 MiB, held by every
+ *  GPU that loads the library until exit; a contract whose grids need more
+ *  (large n_s x n_v) is rejected with FPE_NOALLOC_ERR_SIZE and its status
+ *  slots set to FPE_STATUS_CAPACITY.  The first call on a device resolves the
+ *  array's device address (make it before any stream capture).  Calls share
+ *  the array: overlapping calls on one device race and must be serialized by
+ *  the caller.  prices / status hold n_strikes values (host memory); knock-ins
+ *  use in-out parity; opt->greeks must be 0.  Runs on cuda_stream (NULL: the
+ *  library's stream) and waits for it.  Returns 0, a status code, or < 0. */
+extern int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatchOptions* opt,
+                                 double* prices, int32_t* status, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
