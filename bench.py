@@ -38,7 +38,7 @@ REF_RTOL = 1e-10  # FP64 reference run used to state the error
 
 
 def make_batch(n: int, seed: int):
-    """Config-1 parameter draws: (n, 12) float + (n, 3) int tables."""
+    """Seeded Heston contract draws: (n, 12) float + (n, 3) int tables."""
     rng = np.random.default_rng(seed)
     P = np.zeros((n, 12))
     I = np.zeros((n, 3), np.int32)
@@ -141,14 +141,15 @@ def run_reference_arm(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    P, I = make_batch(N_CONTRACTS, args.seed)
+    nc = args.contracts
+    P, I = make_batch(nc, args.seed)
     cores = os.cpu_count() or 1
-    sample = max(cores, min(args.cpu_sample, N_CONTRACTS))
+    sample = max(cores, min(args.cpu_sample, nc))
     rates = []
     for _ in range(args.warmup):
         cpu_baseline_run(P, I, args.rtol, cores, min(sample, cores))
     for s in range(args.steps):
-        sl = (np.arange(sample) + s * sample) % N_CONTRACTS
+        sl = (np.arange(sample) + s * sample) % nc
         r, _ = cpu_baseline_run(P[sl], I[sl], args.rtol, cores, sample)
         rates.append(r)
     v = float(np.mean(rates))
@@ -156,7 +157,7 @@ def run_reference_arm(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * sample / v, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "config1 256 European contracts, mixed grids",
+            "config": {"workload": f"{args.contracts} European Heston contracts, mixed grids 32-64 x 16-32",
                        "rtol": args.rtol, "contracts_per_step": sample},
             "cpu_baseline": {"value": v, "unit": "prices/s", "cores": cores, "kind": "port",
                              "sample": f"{sample} contracts of the config-1 batch per step, "
@@ -174,6 +175,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--contracts", type=int, default=N_CONTRACTS,
+                    help="contracts per GPU per step (smaller batches serve profiling)")
     ap.add_argument("--rtol", type=float, default=RTOL)
     ap.add_argument("--precision", type=int, default=1)
     ap.add_argument("--cpu-sample", type=int, default=16)
@@ -202,7 +205,8 @@ def main():
 
     if not fpe.is_available():
         raise RuntimeError("CUDA engine unavailable")
-    P, I = make_batch(N_CONTRACTS, args.seed + rank)
+    nc = args.contracts
+    P, I = make_batch(nc, args.seed + rank)
     opts = fpe.BatchOptions(disc=1, precision=args.precision, rtol=args.rtol,
                             atol=args.rtol * 1e-2, complex_solve=2, radau_constants=2)
     arr, keep = fpe.contracts_from_arrays(P, I)
@@ -246,13 +250,13 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
-    value = world * N_CONTRACTS * args.steps / (ms / 1000.0)
+    value = world * nc * args.steps / (ms / 1000.0)
     # ---- end to end through the public C ABI (host contracts -> host prices) -----
-    pinned = torch.empty((N_CONTRACTS, 12), dtype=torch.float64).pin_memory()
+    pinned = torch.empty((nc, 12), dtype=torch.float64).pin_memory()
     pinned.copy_(torch.from_numpy(P))
     Ph = pinned.numpy()
-    h2d = N_CONTRACTS * (C_SIZE_CONTRACT()) + N_CONTRACTS * 8
-    d2h = N_CONTRACTS * 8 + stats["solves"] * 80
+    h2d = nc * (C_SIZE_CONTRACT()) + nc * 8
+    d2h = nc * 8 + stats["solves"] * 80
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -269,7 +273,7 @@ def main():
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = world * N_CONTRACTS * args.steps / e2e_s
+    e2e = world * nc * args.steps / e2e_s
     # ---- roofline of k_radau -----------------------------------------------------
     peak, peak_kind = load_peaks()
     radau_ms = ktimes[3]
@@ -279,7 +283,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        sample = max(min(cores, N_CONTRACTS), min(args.cpu_sample, N_CONTRACTS))
+        sample = max(min(cores, nc), min(args.cpu_sample, nc))
         rate, dt = cpu_baseline_run(P, I, args.rtol, cores, sample)
         cpu = {"value": rate, "unit": "prices/s", "cores": cores, "kind": "port",
                "sample": f"first {sample} contracts of the same batch, oracle C++ FP64 "
@@ -290,7 +294,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32-factors/f64" if args.precision == 1 else "f64", "data": "synthetic",
-            "config": {"workload": "config1: 256 European Heston contracts per GPU, mixed grids "
+            "config": {"workload": f"{nc} European Heston contracts per GPU, mixed grids "
                                    "32-64 x 16-32, one launch sequence",
                        "rtol": args.rtol, "atol": args.rtol * 1e-2, "precision": args.precision,
                        "complex_stage": "direct block LU", "radau_constants": "exact",
