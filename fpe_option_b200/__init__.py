@@ -509,7 +509,7 @@ class Plan:
         keys = ["solves", "accepted", "rejected", "newton", "gmres", "lu", "admm",
                 "max_ndof_s", "max_ndof_v", "total_dofs", "passes_real", "passes_complex",
                 "factor_bytes", "worst_status", "kcyc_factor", "kcyc_solve", "kcyc_kron",
-                "kcyc_total"]
+                "kcyc_total", "kcyc_factor_gj", "kcyc_factor_gemm"]
         return dict(zip(keys, list(out)))
 
     def kernel_times(self, stream: int | None = None) -> list[float]:

@@ -17,6 +17,7 @@
 // systems store interleaved (re, im) pairs.
 #pragma once
 #include "dev_common.cuh"
+#include "bulk_pipe.cuh"
 
 namespace fpe {
 
@@ -101,27 +102,33 @@ struct OpFactors {
   const double *Av, *B1, *B2, *B3, *B4; // v
 };
 
+// Block-banded storage of one stage matrix: block row i holds 7 blocks of
+// nv x nv, kk = 0..6 for block columns i - 3 .. i + 3, each at a stride of
+// fpe_block_stride(nv) elements.  Before and during the factorization a block
+// is row-major; the final factor blocks (L in kk 0-2, P^-1 in kk 3, W = P^-1 U
+// in kk 4-6) are stored transposed (element (j, m) at m nv + j), so that the
+// sweeps read each block column-wise with one output row per thread.
 template <typename ET>
 struct BlockLU {
   ET* F;
-  int ns, nv;
-  __device__ __forceinline__ ET* blk(int i, int kk) const { return F + (size_t(i) * 7 + kk) * nv * nv; }
+  int ns, nv, bs;
+  __device__ __forceinline__ ET* blk(int i, int kk) const { return F + (size_t(i) * 7 + kk) * bs; }
 };
 
 // E = (a_re + i a_im) M + h K into the block storage (a_im ignored for real ET).
 template <typename ET>
 __device__ void blu_assemble(const OpFactors& O, const BlockLU<ET>& L, double a_re, double a_im,
                              double h) {
-  const int ns = O.ns, nv = O.nv;
-  const size_t total = size_t(ns) * 7 * nv * nv;
+  const int ns = O.ns, nv = O.nv, bs = L.bs;
+  const size_t total = size_t(ns) * 7 * bs;
   for (size_t e = threadIdx.x; e < total; e += blockDim.x) {
-    const int jl = int(e % (nv * nv));
-    const int ikk = int(e / (nv * nv));
+    const int jl = int(e % bs);
+    const int ikk = int(e / bs);
     const int i = ikk / 7, kk = ikk - i * 7;
-    const int j = jl / nv, l = jl - j * nv;
+    const int j = jl / nv, l = jl - j * nv;  // j >= nv: block padding
     const int k = i + kk - 3, dl = l - j + 3;
     double m = 0.0, kv = 0.0;
-    if (k >= 0 && k < ns && dl >= 0 && dl < 7) {
+    if (j < nv && k >= 0 && k < ns && dl >= 0 && dl < 7) {
       const int sb = i * 7 + kk, vb = j * 7 + dl;
       m = O.As[sb] * O.Av[vb];
       kv = O.Ss[sb] * O.B1[vb] + O.Ts[sb] * O.B2[vb] + O.As[sb] * O.B3[vb] + O.St[sb] * O.B4[vb];
@@ -187,232 +194,347 @@ __device__ __forceinline__ double fmag(Cx<T> a) {
   return sqrt(double(a.re) * double(a.re) + double(a.im) * double(a.im));
 }
 
-// Shared scratch (in ET elements) needed by blu_factor for block size nv: the
-// augmented pivot block [P | I] (row stride 2 nv + 1), the inverse P^-1, the
-// staged E_{r,i} and U_{i,c} blocks and the computed L_{r,i} blocks, plus the
-// Gauss-Jordan bookkeeping.
-__host__ __device__ __forceinline__ int blu_smem_elems(int nv) {
-  return nv * (2 * nv + 1) + 10 * nv * nv + 4 * nv + 16;
-}
-
-// 2 x 2 register tile of C = A B (nv x nv operands, row strides lda / ldb),
-// rows j0, j0 + 1 and columns l0, l0 + 1 (guarded at odd edges).
-template <typename ET>
-__device__ __forceinline__ void tile2x2(const ET* A_, int lda, const ET* B_, int ldb, int nv, int j0,
-                                        int l0, ET (&acc)[2][2]) {
-  acc[0][0] = acc[0][1] = acc[1][0] = acc[1][1] = fzero(ET());
-  const int j1 = min(j0 + 1, nv - 1), l1 = min(l0 + 1, nv - 1);
-#pragma unroll 4
-  for (int m = 0; m < nv; ++m) {
-    const ET a0 = A_[j0 * lda + m], a1 = A_[j1 * lda + m];
-    const ET b0 = B_[m * ldb + l0], b1 = B_[m * ldb + l1];
-    ffma(acc[0][0], a0, b0);
-    ffma(acc[0][1], a0, b1);
-    ffma(acc[1][0], a1, b0);
-    ffma(acc[1][1], a1, b1);
-  }
-}
-
-// Shared (or global) factorization scratch of one system.
+// --------------------------------------------------------------------------
+// Stage-matrix factorization scratch (one system, ET elements).
+//
+// Blocks are staged with a padded width nvp = nv rounded up to 4 so that every
+// tile operand is a 16-byte vector load.  GEMM left operands are stored
+// transposed (k-major, row stride ldt = nvp + 4: the transposed staging
+// writes spread over 8 banks), right operands row-major (stride nvp).
+//   aug  nv x (nv + 1)   in-place Gauss-Jordan array of the pivot block
+//   Pi   nvp x nvp       P^-1, row-major        (right operand of L = E P^-1)
+//   PiT  nvp x ldt       P^-1, transposed       (left operand of W = P^-1 U)
+//   EbT  3 x nvp x ldt   E_{i+1+r, i}, transposed
+//   LbT  3 x nvp x ldt   L_{i+1+r, i} = E P^-1, transposed (left operand of the Schur update)
+//   Ub   3 x nvp x nvp   U_{i, i+1+c}, row-major
+//   pinv nvp (inverse pivot of each column), then the pivot rows prow_of and
+//   their columns q_of (int)
+// --------------------------------------------------------------------------
 template <typename ET>
 struct FacScratch {
-  ET *aug, *Pi, *Eb, *Lb, *Ub;
-  ET* fcol[2];   // elimination factors, double-buffered across columns
+  ET *aug, *Pi, *PiT, *EbT, *LbT, *Ub;
+  ET* pinv;      // inverse pivot value of each column
   int* prow_of;  // pivot row of each column
-  int* used;     // row already pivotal
-  int* ctl;      // [0], [1]: pivot row of the current / next column
-  int nv, w1, nn;
+  int* q_of;     // column whose pivot row is r
+  int nv, nvp, ldt, w1;
+  bool shared;   // scratch in shared memory (async staging possible)
   __device__ void init(ET* base, int nv_) {
     nv = nv_;
-    w1 = 2 * nv + 1;
-    nn = nv * nv;
+    shared = __isShared(base) != 0;
+    nvp = fpe_fac_nvp(nv);
+    ldt = nvp + 4;
+    w1 = nv + 1;
+    const int p = nvp, t = ldt;
     aug = base;
-    Pi = aug + nv * w1;
-    Eb = Pi + nn;
-    Lb = Eb + 3 * nn;
-    Ub = Lb + 3 * nn;
-    fcol[0] = Ub + 3 * nn;
-    fcol[1] = fcol[0] + nv;
-    prow_of = reinterpret_cast<int*>(fcol[1] + nv);
-    used = prow_of + nv;
-    ctl = used + nv;
+    Pi = aug + ((nv * (nv + 1) + 3) & ~3);
+    PiT = Pi + p * p;
+    EbT = PiT + p * t;
+    LbT = EbT + 3 * p * t;
+    Ub = LbT + 3 * p * t;
+    pinv = Ub + 3 * p * p;
+    prow_of = reinterpret_cast<int*>(pinv + p);
+    q_of = prow_of + p;
   }
 };
 
-// Scratch (ET elements) per system for block size nv.
-__host__ __device__ __forceinline__ int blu_smem_elems_v2(int nv) {
-  return nv * (2 * nv + 1) + 10 * nv * nv + 6 * nv + 16;
+// ---- register tiles ------------------------------------------------------
+// Tile shape per element type: 4 x 4 real, 2 x 4 complex (16 FMA lanes of
+// real arithmetic per operand pair either way).
+template <typename ET>
+struct TileM { static constexpr int v = 4; };
+template <typename T>
+struct TileM<Cx<T>> { static constexpr int v = 2; };
+constexpr int kTileN = 4;
+
+// Vector loads/stores of K consecutive elements from 16-byte aligned shared memory.
+template <int K>
+__device__ __forceinline__ void vld(const float* p, float (&o)[K]) {
+#pragma unroll
+  for (int q = 0; q < K; q += 4) {
+    const float4 v = *reinterpret_cast<const float4*>(p + q);
+    o[q] = v.x; o[q + 1] = v.y; o[q + 2] = v.z; o[q + 3] = v.w;
+  }
+}
+template <int K>
+__device__ __forceinline__ void vld(const double* p, double (&o)[K]) {
+#pragma unroll
+  for (int q = 0; q < K; q += 2) {
+    const double2 v = *reinterpret_cast<const double2*>(p + q);
+    o[q] = v.x; o[q + 1] = v.y;
+  }
+}
+template <int K>
+__device__ __forceinline__ void vld(const Cx<float>* p, Cx<float> (&o)[K]) {
+#pragma unroll
+  for (int q = 0; q < K; q += 2) {
+    const float4 v = *reinterpret_cast<const float4*>(p + q);
+    o[q] = cmk(v.x, v.y); o[q + 1] = cmk(v.z, v.w);
+  }
+}
+template <int K>
+__device__ __forceinline__ void vld(const Cx<double>* p, Cx<double> (&o)[K]) {
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    const double2 v = *reinterpret_cast<const double2*>(p + q);
+    o[q] = cmk(v.x, v.y);
+  }
+}
+template <typename ET, int K>
+__device__ __forceinline__ void vst(ET* p, const ET (&v)[K]) {
+#pragma unroll
+  for (int q = 0; q < K; ++q) p[q] = v[q];
+}
+
+__device__ __forceinline__ void ffms(float& a, float x, float y) { a = fmaf(-x, y, a); }
+__device__ __forceinline__ void ffms(double& a, double x, double y) { a = fma(-x, y, a); }
+template <typename T>
+__device__ __forceinline__ void ffms(Cx<T>& a, Cx<T> x, Cx<T> y) {
+  a.re = fma(-x.re, y.re, a.re);
+  a.re = fma(x.im, y.im, a.re);
+  a.im = fma(-x.re, y.im, a.im);
+  a.im = fma(-x.im, y.re, a.im);
+}
+
+// acc (+)= sum_k AT[k][j0 + m] B[k][l0 + n], k < K  (SUB: acc -= ...)
+template <typename ET, bool SUB>
+__device__ __forceinline__ void tile_mm(const ET* AT, int lda, const ET* B, int ldb, int K, int j0, int l0,
+                                        ET (&acc)[TileM<ET>::v][kTileN]) {
+  constexpr int TM = TileM<ET>::v;
+  const ET* pa = AT + j0;
+  const ET* pb = B + l0;
+#pragma unroll 2
+  for (int k = 0; k < K; ++k) {
+    ET a[TM], b[kTileN];
+    vld<TM>(pa + k * lda, a);
+    vld<kTileN>(pb + k * ldb, b);
+#pragma unroll
+    for (int m = 0; m < TM; ++m)
+#pragma unroll
+      for (int n = 0; n < kTileN; ++n) {
+        if constexpr (SUB) ffms(acc[m][n], a[m], b[n]);
+        else ffma(acc[m][n], a[m], b[n]);
+      }
+  }
+}
+
+// ---- per block row steps ----------------------------------------------------
+// Row and column of element e of an nv-wide block without an integer
+// division: (e + 1/2) / nv rounded down is exact for e < 2^16.
+__device__ __forceinline__ void rc_of(int e, int nv, float rnv, int& r, int& c) {
+  r = int((float(e) + 0.5f) * rnv);
+  c = e - r * nv;
+}
+
+// Stage block row i into the scratch: the pivot block into the Gauss-Jordan
+// array, U_{i,i+1+c} row-major and E_{i+1+r,i} transposed.  With the scratch
+// in shared memory the elements move by per-element asynchronous copies that
+// are all in flight together; a global-memory scratch (blocks too wide for
+// shared memory) is filled by ordinary loads and stores.  The caller's barrier
+// follows.
+template <typename ET, bool ASYNC>
+__device__ __forceinline__ void stage_elem(ET* dst, const ET* src) {
+  if constexpr (ASYNC) {
+    cp_async_elem<int(sizeof(ET))>(dst, src);
+  } else {
+    *dst = *src;
+  }
+}
+
+template <typename ET, bool ASYNC>
+__device__ void fac_stage_impl(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
+  const int nv = S.nv, nn = nv * nv, w1 = S.w1, p = S.nvp, t = S.ldt;
+  const float rnv = 1.0f / float(nv);
+  const ET* P = L.blk(i, 3);
+  for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+    int r, c;
+    rc_of(e, nv, rnv, r, c);
+    stage_elem<ET, ASYNC>(S.aug + r * w1 + c, P + e);
+  }
+  for (int cc = 0; cc < nr; ++cc) {
+    const ET* U = L.blk(i, 4 + cc);
+    const ET* E = L.blk(i + 1 + cc, 2 - cc);
+    ET* ub = S.Ub + cc * p * p;
+    ET* et = S.EbT + cc * p * t;
+    for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+      int j, l;
+      rc_of(e, nv, rnv, j, l);
+      stage_elem<ET, ASYNC>(ub + j * p + l, U + e);
+      stage_elem<ET, ASYNC>(et + l * t + j, E + e);
+    }
+  }
+  for (int r = threadIdx.x; r < nv; r += blockDim.x) {
+    S.q_of[r] = r;  // stays a valid column index even if a pivot search fails
+    S.prow_of[r] = r;
+  }
+  if constexpr (ASYNC) cp_async_wait_all();
 }
 
 template <typename ET>
 __device__ void fac_stage(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
-  const int nv = S.nv, nn = S.nn, w1 = S.w1;
-  const ET* P = L.blk(i, 3);
-  for (int e = threadIdx.x; e < nv * 2 * nv; e += blockDim.x) {
-    const int r = e / (2 * nv), c = e - r * (2 * nv);
-    S.aug[r * w1 + c] = c < nv ? P[r * nv + c] : ((c - nv == r) ? fone(ET()) : fzero(ET()));
+  if (S.shared) {
+    fac_stage_impl<ET, true>(L, S, i, nr);
+  } else {
+    fac_stage_impl<ET, false>(L, S, i, nr);
   }
-  for (int e = threadIdx.x; e < nr * nn; e += blockDim.x) {
-    const int cc = e / nn, jl = e - cc * nn;
-    S.Ub[e] = L.blk(i, 4 + cc)[jl];
-    S.Eb[e] = L.blk(i + 1 + cc, 2 - cc)[jl];
-  }
-  for (int r = threadIdx.x; r < nv; r += blockDim.x) S.used[r] = 0;
 }
 
-// Pivot selection for column c by warp `wsel` from the column values v[k]
-// (rows lane + 32 k); writes the elimination factors and the pivot row.
-template <typename ET>
-__device__ __forceinline__ bool fac_pick(FacScratch<ET>& S, int c, const ET (&v)[2], int buf) {
-  const int lane = threadIdx.x & 31, nv = S.nv;
-  double best = -1.0;
-  int bi = nv;
-  for (int k = 0; k < 2; ++k) {
-    const int r = lane + 32 * k;
-    if (r < nv && !S.used[r]) {
-      const double m = fmag(v[k]);
-      if (m > best) {
-        best = m;
-        bi = r;
-      }
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-    if (ob > best || (ob == best && oi < bi)) {
-      best = ob;
-      bi = oi;
-    }
-  }
-  const int p = bi < nv ? bi : c;
-  // broadcast the pivot value from its owning lane
-  ET pv;
-  {
-    const int owner = p & 31, kk = p >> 5;
-    ET mine = v[kk < 2 ? kk : 0];
-    if constexpr (IsCx<ET>::v) {
-      pv.re = __shfl_sync(0xffffffffu, mine.re, owner);
-      pv.im = __shfl_sync(0xffffffffu, mine.im, owner);
-    } else {
-      pv = __shfl_sync(0xffffffffu, mine, owner);
-    }
-  }
-  const ET inv = finv(pv);
-  for (int k = 0; k < 2; ++k) {
-    const int r = lane + 32 * k;
-    if (r < nv) S.fcol[buf][r] = (r == p) ? fzero(ET()) : fmul(v[k], inv);
-  }
-  if (lane == 0) {
-    S.ctl[buf] = p;
-    S.used[p] = 1;
-    S.prow_of[c] = p;
-  }
-  return best > 0.0;
+// |re| + |im| (LAPACK's cabs1) as the pivot magnitude, in float.
+__device__ __forceinline__ float pmag(float a) { return fabsf(a); }
+__device__ __forceinline__ float pmag(double a) { return float(fabs(a)); }
+template <typename T>
+__device__ __forceinline__ float pmag(Cx<T> a) {
+  return float(fabs(double(a.re)) + fabs(double(a.im)));
 }
 
-// Gauss-Jordan elimination of column c (pivot row ctl[c&1]) by the CTA; warp
-// `wsel` owns column c + 1, updates it first and picks its pivot (look-ahead),
-// so each column costs one barrier.
+// Pivot key of row r: the magnitude's float bits above bit 7, then 127 - r,
+// so one unsigned max over the warp picks the largest magnitude and, among
+// equal keys, the lowest row.  Rows already pivotal have key 0.
+__device__ __forceinline__ unsigned pivot_key(float m, int r) {
+  return (__float_as_uint(m) & ~127u) | unsigned(127 - r);
+}
+
+// In-place Gauss-Jordan inversion of the staged pivot block by one warp, with
+// unscaled pivot rows:  for column c with pivot row p and f_r = a_rc / a_pc,
+//   a_rl -= f_r a_pl (r != p, all l),   a_rc = -f_r (r != p),   a_pc = 1.
+// Lane r owns rows r and r + 32, so a step touches only the lane's own rows
+// and reads the pivot row, which no lane writes during that step.  After the
+// last column, row p_k divided by the pivot a_{p_k k} holds row k of P^-1 with
+// its columns in pivot order (column q_l holds inverse column l).  Returns
+// false for a zero or non-finite pivot.
 template <typename ET>
-__device__ bool fac_elim(FacScratch<ET>& S, int c, int wsel) {
-  const int nv = S.nv, w1 = S.w1, buf = c & 1;
-  const int p = S.ctl[buf];
-  const ET* f = S.fcol[buf];
-  const ET* prow = S.aug + p * w1;
-  bool ok = true;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cn = c + 1;
-  if (warp == wsel && cn < nv) {
-    ET v[2];
-    v[0] = v[1] = fzero(ET());
-    for (int k = 0; k < 2; ++k) {
-      const int r = lane + 32 * k;
-      if (r >= nv) continue;
-      ET& x = S.aug[r * w1 + cn];
-      if (r != p) x = fsub(x, fmul(f[r], prow[cn]));
-      v[k] = x;
+__device__ bool fac_gj_warp(FacScratch<ET>& S) {
+  const int lane = threadIdx.x & 31, nv = S.nv, w1 = S.w1;
+  const int r0 = lane, r1 = lane + 32;
+  const bool own0 = r0 < nv, own1 = r1 < nv;
+  bool used0 = false, used1 = false, ok = true;
+  ET* a0 = S.aug + r0 * w1;
+  ET* a1 = S.aug + r1 * w1;
+  for (int c = 0; c < nv; ++c) {
+    unsigned k = 0;
+    if (own0 && !used0) k = pivot_key(pmag(a0[c]), r0);
+    if (own1 && !used1) k = max(k, pivot_key(pmag(a1[c]), r1));
+    const unsigned kmax = __reduce_max_sync(0xffffffffu, k);
+    const int p = min(127 - int(kmax & 127u), nv - 1);  // an unused row always has a nonzero key
+    const ET* ap = S.aug + p * w1;
+    const ET pv = ap[c];
+    const float pm = pmag(pv);
+    ok &= (pm > 0.f) && (pm < CUDART_INF_F);
+    const ET inv = finv(pv);
+    if (p == r0) used0 = true;
+    if (p == r1) used1 = true;
+    if (lane == 0) {
+      S.prow_of[c] = p;
+      S.q_of[p] = c;
+      S.pinv[c] = inv;
     }
-    ok = fac_pick<ET>(S, cn, v, buf ^ 1);
-  }
-  const int skip = cn < nv ? cn : -1;  // column already updated by the look-ahead warp
-  for (int e = threadIdx.x; e < nv * 2 * nv; e += blockDim.x) {
-    const int r = e / (2 * nv), l = e - r * (2 * nv);
-    if (r == p || l == skip) continue;
-    ET& x = S.aug[r * w1 + l];
-    x = fsub(x, fmul(f[r], prow[l]));
+    __syncwarp();  // every lane has read a_pc before the owner overwrites it
+    if (own0 && r0 != p) {
+      const ET f = fmul(a0[c], inv);
+#pragma unroll 4
+      for (int l = 0; l < nv; ++l) a0[l] = fsub(a0[l], fmul(f, ap[l]));
+      a0[c] = fsub(fzero(ET()), f);
+    }
+    if (own1 && r1 != p) {
+      const ET f = fmul(a1[c], inv);
+#pragma unroll 4
+      for (int l = 0; l < nv; ++l) a1[l] = fsub(a1[l], fmul(f, ap[l]));
+      a1[c] = fsub(fzero(ET()), f);
+    }
+    if (p == r0) a0[c] = fone(ET());
+    if (p == r1) a1[c] = fone(ET());
+    __syncwarp();
   }
   return ok;
 }
 
+// P^-1 (row k = row p_k of the array scaled by 1 / a_{p_k k}, columns
+// un-permuted) into Pi, PiT and the factor storage.
 template <typename ET>
 __device__ void fac_extract(const BlockLU<ET>& L, FacScratch<ET>& S, int i) {
-  const int nv = S.nv, w1 = S.w1;
-  for (int e = threadIdx.x; e < S.nn; e += blockDim.x) {
-    const int c = e / nv, l = e - c * nv;
-    const int p = S.prow_of[c];
-    const ET v = fmul(S.aug[p * w1 + nv + l], finv(S.aug[p * w1 + c]));
-    S.Pi[e] = v;
-    L.blk(i, 3)[e] = v;
+  const int nv = S.nv, w1 = S.w1, p = S.nvp, t = S.ldt;
+  ET* g = L.blk(i, 3);
+  for (int e = threadIdx.x; e < nv * nv; e += blockDim.x) {
+    const int k = e / nv, l = e - k * nv;
+    const ET v = fmul(S.aug[S.prow_of[k] * w1 + S.q_of[l]], S.pinv[k]);
+    S.Pi[k * p + l] = v;
+    S.PiT[l * t + k] = v;
+    g[l * nv + k] = v;  // stored transposed
   }
 }
 
-// L_ri = E_ri P^-1 (shared), W_ic = P^-1 U_ic (global)
+// L_r = E_r P^-1 (transposed to the factor storage and to LbT) and
+// W_c = P^-1 U_c (transposed to the factor storage), r, c < nr.
 template <typename ET>
 __device__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
-  const int nv = S.nv, nn = S.nn, th = (nv + 1) / 2, ntile = th * th;
-  for (int t = threadIdx.x; t < 2 * nr * ntile; t += blockDim.x) {
-    const int job = t / ntile, tt = t - job * ntile;
-    const int j0 = 2 * (tt / th), l0 = 2 * (tt - (tt / th) * th);
-    ET acc[2][2];
+  constexpr int TM = TileM<ET>::v;
+  const int nv = S.nv, p = S.nvp, t = S.ldt;
+  const int tr = p / TM, tc = p / kTileN, ntile = tr * tc;
+  for (int q = threadIdx.x; q < 2 * nr * ntile; q += blockDim.x) {
+    const int job = q / ntile, tt = q - job * ntile;
+    const int j0 = (tt / tc) * TM, l0 = (tt - (tt / tc) * tc) * kTileN;
+    ET acc[TM][kTileN];
+#pragma unroll
+    for (int m = 0; m < TM; ++m)
+#pragma unroll
+      for (int n = 0; n < kTileN; ++n) acc[m][n] = fzero(ET());
+    ET* dst;
     if (job < nr) {
-      tile2x2<ET>(S.Eb + job * nn, nv, S.Pi, nv, nv, j0, l0, acc);
-      ET* dst = S.Lb + job * nn;
-      for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < 2; ++b)
-          if (j0 + a < nv && l0 + b < nv) dst[(j0 + a) * nv + l0 + b] = acc[a][b];
+      tile_mm<ET, false>(S.EbT + job * p * t, t, S.Pi, p, nv, j0, l0, acc);
+      dst = L.blk(i + 1 + job, 2 - job);
+      ET* lt = S.LbT + job * p * t;
+#pragma unroll
+      for (int n = 0; n < kTileN; ++n) {
+        ET col[TM];
+#pragma unroll
+        for (int m = 0; m < TM; ++m) col[m] = acc[m][n];
+        vst<ET, TM>(lt + (l0 + n) * t + j0, col);
+      }
     } else {
       const int cc = job - nr;
-      tile2x2<ET>(S.Pi, nv, S.Ub + cc * nn, nv, nv, j0, l0, acc);
-      ET* W = L.blk(i, 4 + cc);
-      for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < 2; ++b)
-          if (j0 + a < nv && l0 + b < nv) W[(j0 + a) * nv + l0 + b] = acc[a][b];
+      tile_mm<ET, false>(S.PiT, t, S.Ub + cc * p * p, p, nv, j0, l0, acc);
+      dst = L.blk(i, 4 + cc);
     }
+#pragma unroll
+    for (int m = 0; m < TM; ++m)
+#pragma unroll
+      for (int n = 0; n < kTileN; ++n)
+        if (j0 + m < nv && l0 + n < nv) dst[(l0 + n) * nv + j0 + m] = acc[m][n];
   }
 }
 
-// L blocks out; E_rc -= L_ri U_ic
+// Schur update E_{i+1+r, i+1+c} -= L_r U_c in the factor storage (r, c < nr);
+// the target tile is loaded first so its latency overlaps the products.
 template <typename ET>
 __device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
-  const int nv = S.nv, nn = S.nn, th = (nv + 1) / 2, ntile = th * th;
-  for (int e = threadIdx.x; e < nr * nn; e += blockDim.x) {
-    const int rr = e / nn, jl = e - rr * nn;
-    L.blk(i + 1 + rr, 2 - rr)[jl] = S.Lb[e];
-  }
-  for (int t = threadIdx.x; t < nr * nr * ntile; t += blockDim.x) {
-    const int job = t / ntile, tt = t - job * ntile;
-    const int j0 = 2 * (tt / th), l0 = 2 * (tt - (tt / th) * th);
+  constexpr int TM = TileM<ET>::v;
+  const int nv = S.nv, p = S.nvp, t = S.ldt;
+  const int tr = p / TM, tc = p / kTileN, ntile = tr * tc;
+  for (int q = threadIdx.x; q < nr * nr * ntile; q += blockDim.x) {
+    const int job = q / ntile, tt = q - job * ntile;
+    const int j0 = (tt / tc) * TM, l0 = (tt - (tt / tc) * tc) * kTileN;
     const int rr = job / nr, cc = job - rr * nr;
-    ET acc[2][2];
-    tile2x2<ET>(S.Lb + rr * nn, nv, S.Ub + cc * nn, nv, nv, j0, l0, acc);
     ET* E = L.blk(i + 1 + rr, cc - rr + 3);
-    for (int a = 0; a < 2; ++a)
-      for (int b = 0; b < 2; ++b)
-        if (j0 + a < nv && l0 + b < nv) {
-          ET& x = E[(j0 + a) * nv + l0 + b];
-          x = fsub(x, acc[a][b]);
-        }
+    ET acc[TM][kTileN];
+#pragma unroll
+    for (int m = 0; m < TM; ++m)
+#pragma unroll
+      for (int n = 0; n < kTileN; ++n)
+        acc[m][n] = (j0 + m < nv && l0 + n < nv) ? E[(j0 + m) * nv + l0 + n] : fzero(ET());
+    tile_mm<ET, true>(S.LbT + rr * p * t, t, S.Ub + cc * p * p, p, nv, j0, l0, acc);
+#pragma unroll
+    for (int m = 0; m < TM; ++m)
+#pragma unroll
+      for (int n = 0; n < kTileN; ++n)
+        if (j0 + m < nv && l0 + n < nv) E[(j0 + m) * nv + l0 + n] = acc[m][n];
   }
 }
 
 // Factor the real stage matrix (and, when LC is given, the complex one in
 // lockstep so both share every barrier).  scr_r / scr_c: scratch of
-// blu_smem_elems_v2(nv) elements each.
+// fpe_fac_scratch_elems(nv) elements each.
 template <typename FT>
 __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC, FT* scr_r,
-                                Cx<FT>* scr_c) {
+                                Cx<FT>* scr_c, long long (&tcyc)[2]) {
   const int ns = LR.ns, nv = LR.nv;
   FacScratch<FT> SR;
   SR.init(scr_r, nv);
@@ -425,43 +547,27 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
     fac_stage<FT>(LR, SR, i, nr);
     if (LC) fac_stage<Cx<FT>>(*LC, SC, i, nr);
     __syncthreads();
-    // pivots of column 0 (warp 0: real, warp 1: complex)
-    if (warp == 0) {
-      FT v[2];
-      v[0] = v[1] = fzero(FT());
-      for (int k = 0; k < 2; ++k) {
-        const int r = (threadIdx.x & 31) + 32 * k;
-        if (r < nv) v[k] = SR.aug[r * SR.w1];
-      }
-      ok &= fac_pick<FT>(SR, 0, v, 0);
-    } else if (warp == 1 && LC) {
-      Cx<FT> v[2];
-      v[0] = v[1] = fzero(Cx<FT>());
-      for (int k = 0; k < 2; ++k) {
-        const int r = (threadIdx.x & 31) + 32 * k;
-        if (r < nv) v[k] = SC.aug[r * SC.w1];
-      }
-      ok &= fac_pick<Cx<FT>>(SC, 0, v, 0);
-    }
+    // pivot-block inverses: warp 0 real, warp 1 complex, concurrently
+    const long long t0 = clock64();
+    if (warp == 0) ok &= fac_gj_warp<FT>(SR);
+    else if (warp == 1 && LC) ok &= fac_gj_warp<Cx<FT>>(SC);
     __syncthreads();
-    for (int c = 0; c < nv; ++c) {
-      ok &= fac_elim<FT>(SR, c, 0);
-      if (LC) ok &= fac_elim<Cx<FT>>(SC, c, 1);
-      __syncthreads();
-    }
+    tcyc[0] += clock64() - t0;
     fac_extract<FT>(LR, SR, i);
     if (LC) fac_extract<Cx<FT>>(*LC, SC, i);
     __syncthreads();
     if (nr > 0) {
+      const long long t2 = clock64();
       fac_lw<FT>(LR, SR, i, nr);
       if (LC) fac_lw<Cx<FT>>(*LC, SC, i, nr);
       __syncthreads();
       fac_update<FT>(LR, SR, i, nr);
       if (LC) fac_update<Cx<FT>>(*LC, SC, i, nr);
       __syncthreads();
+      tcyc[1] += clock64() - t2;
     }
   }
-  return ok;
+  return __syncthreads_and(ok ? 1 : 0) != 0;  // the same verdict in every thread
 }
 
 // Right-hand sides of one fused solve: up to two real vectors on the real
@@ -480,35 +586,37 @@ struct SolveSet {
   int nc;  // 0 or 1
 };
 
+// Dot product of row j of a stored (transposed) factor block with x over the
+// lanes gl, gl + G, ... of a group: col = block + j, element m at col[m nv].
 template <typename ET, typename A>
-__device__ __forceinline__ A grp_dot(const ET* row, const double* xre, const double* xim, int nv, int gl, int G);
+__device__ __forceinline__ A grp_dot(const ET* col, const double* xre, const double* xim, int nv, int gl, int G);
 
 template <>
-__device__ __forceinline__ double grp_dot<float, double>(const float* row, const double* x, const double*, int nv,
+__device__ __forceinline__ double grp_dot<float, double>(const float* col, const double* x, const double*, int nv,
                                                          int gl, int G) {
   double a = 0.0;
-  for (int m = gl; m < nv; m += G) a = fma(double(row[m]), x[m], a);
+  for (int m = gl; m < nv; m += G) a = fma(double(col[m * nv]), x[m], a);
   return a;
 }
 template <>
-__device__ __forceinline__ double grp_dot<double, double>(const double* row, const double* x, const double*,
+__device__ __forceinline__ double grp_dot<double, double>(const double* col, const double* x, const double*,
                                                           int nv, int gl, int G) {
   double a = 0.0;
-  for (int m = gl; m < nv; m += G) a = fma(row[m], x[m], a);
+  for (int m = gl; m < nv; m += G) a = fma(col[m * nv], x[m], a);
   return a;
 }
 template <>
-__device__ __forceinline__ Cx<double> grp_dot<Cx<float>, Cx<double>>(const Cx<float>* row, const double* xr,
+__device__ __forceinline__ Cx<double> grp_dot<Cx<float>, Cx<double>>(const Cx<float>* col, const double* xr,
                                                                       const double* xi, int nv, int gl, int G) {
   Cx<double> a = cmk(0.0, 0.0);
-  for (int m = gl; m < nv; m += G) afma(a, acc_load(row[m]), cmk(xr[m], xi[m]));
+  for (int m = gl; m < nv; m += G) afma(a, acc_load(col[m * nv]), cmk(xr[m], xi[m]));
   return a;
 }
 template <>
-__device__ __forceinline__ Cx<double> grp_dot<Cx<double>, Cx<double>>(const Cx<double>* row, const double* xr,
+__device__ __forceinline__ Cx<double> grp_dot<Cx<double>, Cx<double>>(const Cx<double>* col, const double* xr,
                                                                        const double* xi, int nv, int gl, int G) {
   Cx<double> a = cmk(0.0, 0.0);
-  for (int m = gl; m < nv; m += G) afma(a, row[m], cmk(xr[m], xi[m]));
+  for (int m = gl; m < nv; m += G) afma(a, col[m * nv], cmk(xr[m], xi[m]));
   return a;
 }
 
@@ -544,19 +652,19 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
       const double* x = S.xr[sys];
       if (i < ns)
         for (int k = 1; k <= 3 && i - k >= 0; ++k)
-          ar += grp_dot<FT, double>(L.blk(i, 3 - k) + j * nv, x + (i - k) * nv, nullptr, nv, gl, G);
-      if (i > 0) zr = grp_dot<FT, double>(L.blk(i - 1, 3) + j * nv, x + (i - 1) * nv, nullptr, nv, gl, G);
+          ar += grp_dot<FT, double>(L.blk(i, 3 - k) + j, x + (i - k) * nv, nullptr, nv, gl, G);
+      if (i > 0) zr = grp_dot<FT, double>(L.blk(i - 1, 3) + j, x + (i - 1) * nv, nullptr, nv, gl, G);
     } else if (is_c) {
       const BlockLU<Cx<FT>>& L = *S.Cf;
       if (i < ns)
         for (int k = 1; k <= 3 && i - k >= 0; ++k) {
-          const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i, 3 - k) + j * nv, S.xc_re + (i - k) * nv,
+          const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i, 3 - k) + j, S.xc_re + (i - k) * nv,
                                                            S.xc_im + (i - k) * nv, nv, gl, G);
           ar += d.re;
           ai += d.im;
         }
       if (i > 0) {
-        const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i - 1, 3) + j * nv, S.xc_re + (i - 1) * nv,
+        const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i - 1, 3) + j, S.xc_re + (i - 1) * nv,
                                                          S.xc_im + (i - 1) * nv, nv, gl, G);
         zr = d.re;
         zi = d.im;
@@ -587,11 +695,11 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
       const BlockLU<FT>& L = *S.R;
       const double* x = S.xr[sys];
       for (int k = 1; k <= 3 && i + k < ns; ++k)
-        ar += grp_dot<FT, double>(L.blk(i, 3 + k) + j * nv, x + (i + k) * nv, nullptr, nv, gl, G);
+        ar += grp_dot<FT, double>(L.blk(i, 3 + k) + j, x + (i + k) * nv, nullptr, nv, gl, G);
     } else if (is_c) {
       const BlockLU<Cx<FT>>& L = *S.Cf;
       for (int k = 1; k <= 3 && i + k < ns; ++k) {
-        const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i, 3 + k) + j * nv, S.xc_re + (i + k) * nv,
+        const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i, 3 + k) + j, S.xc_re + (i + k) * nv,
                                                          S.xc_im + (i + k) * nv, nv, gl, G);
         ar += d.re;
         ai += d.im;
@@ -608,6 +716,255 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
     }
     __syncthreads();
   }
+}
+
+
+// --------------------------------------------------------------------------
+// Staged fused block solve.
+//
+// The 2 ns + 1 block rows of a solve (forward rows 0..ns, backward rows
+// ns-1..0) stream through two shared-memory stage buffers by bulk copies:
+// while the CTA multiplies stage s, stage s + 1 is in flight, and thread 0
+// issues stage s + 2 into the freed buffer after the row's barrier.  A stage
+// holds the blocks the row needs from each factor (forward row i: L_{i,i-3+g},
+// g < 3, and P^-1_{i-1}; backward row i: W_{i,i+1+g}), one slot per block with
+// a 64-byte gap so that the slots of a complex row group start in alternate
+// bank halves.  The last four solved block segments of every right-hand side
+// stay in a shared ring, so each row reads its x operands from shared memory.
+// One thread owns one row of a real system; Gc lanes own one row of the
+// complex system and split its blocks.
+// --------------------------------------------------------------------------
+struct SolveStage {
+  unsigned char* buf[2];     // stage buffers (shared, 16-byte aligned)
+  double* ring;              // 4 segments x nv per right-hand-side array (nr real, re, im)
+  unsigned long long* bar;   // 2 mbarriers (shared)
+  int* err;                  // shared flag: a bounded wait gave up
+  int slot_r, slot_c;        // bytes per staged real / complex block slot
+};
+
+__host__ __device__ __forceinline__ int stage_slot_bytes(int nv, int esz) {
+  return fpe_block_stride(nv) * esz + 64;
+}
+// Bytes of the two stage buffers plus the ring for block size nv, element size
+// esz of the real factor, with or without the complex factor.
+__host__ __device__ __forceinline__ int stage_total_bytes(int nv, int esz, bool cplx) {
+  const int stage = 4 * stage_slot_bytes(nv, esz) + (cplx ? 4 * stage_slot_bytes(nv, 2 * esz) : 0);
+  return 2 * stage + 4 * nv * 4 * 8;
+}
+
+// Block (row, kk) of stage s and slot g; nullptr when the row has no such block.
+template <typename ET>
+__device__ __forceinline__ const ET* stage_block(const BlockLU<ET>& L, int s, int g) {
+  const int ns = L.ns;
+  if (s <= ns) {
+    const int i = s;
+    if (g < 3) return (i < ns && i - 3 + g >= 0) ? L.blk(i, g) : nullptr;
+    return i >= 1 ? L.blk(i - 1, 3) : nullptr;
+  }
+  const int i = 2 * ns - s;
+  return (g < 3 && i + 1 + g < ns) ? L.blk(i, 4 + g) : nullptr;
+}
+
+template <typename FT>
+__device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s) {
+  unsigned long long* bar = P.bar + (s & 1);
+  unsigned char* dst = P.buf[s & 1];
+  const int nv = S.R ? S.R->nv : S.Cf->nv;
+  const uint32_t br = uint32_t(fpe_block_stride(nv)) * sizeof(FT);
+  const uint32_t bc = 2 * br;
+  uint32_t bytes = 0;
+  for (int g = 0; g < 4; ++g) {
+    if (S.nr > 0 && stage_block(*S.R, s, g)) bytes += br;
+    if (S.nc > 0 && stage_block(*S.Cf, s, g)) bytes += bc;
+  }
+  fence_proxy_async_smem();
+  fence_proxy_async_global();
+  if (bytes == 0) {
+    mbar_arrive(bar);
+    return;
+  }
+  mbar_arrive_expect_tx(bar, bytes);
+  for (int g = 0; g < 4; ++g) {
+    if (S.nr > 0) {
+      const FT* src = stage_block(*S.R, s, g);
+      if (src) bulk_g2s(dst + g * P.slot_r, src, br, bar);
+    }
+    if (S.nc > 0) {
+      const Cx<FT>* src = stage_block(*S.Cf, s, g);
+      if (src) bulk_g2s(dst + 4 * P.slot_r + g * P.slot_c, src, bc, bar);
+    }
+  }
+}
+
+// a += sum_m col[m nv] x[m] with two accumulators (col: shared, transposed block)
+__device__ __forceinline__ void col_dot(const float* col, const double* x, int nv, double& a) {
+  double a0 = 0.0, a1 = 0.0;
+  int m = 0;
+  for (; m + 1 < nv; m += 2) {
+    a0 = fma(double(col[m * nv]), x[m], a0);
+    a1 = fma(double(col[(m + 1) * nv]), x[m + 1], a1);
+  }
+  if (m < nv) a0 = fma(double(col[m * nv]), x[m], a0);
+  a += a0 + a1;
+}
+__device__ __forceinline__ void col_dot(const double* col, const double* x, int nv, double& a) {
+  double a0 = 0.0, a1 = 0.0;
+  int m = 0;
+  for (; m + 1 < nv; m += 2) {
+    a0 = fma(col[m * nv], x[m], a0);
+    a1 = fma(col[(m + 1) * nv], x[m + 1], a1);
+  }
+  if (m < nv) a0 = fma(col[m * nv], x[m], a0);
+  a += a0 + a1;
+}
+template <typename T>
+__device__ __forceinline__ void col_dot_c(const Cx<T>* col, const double* xr, const double* xi, int nv, double& ar,
+                                          double& ai) {
+  double r0 = 0.0, i0 = 0.0;
+  for (int m = 0; m < nv; ++m) {
+    const Cx<T> b = col[m * nv];
+    const double br = double(b.re), bi = double(b.im);
+    r0 = fma(br, xr[m], r0);
+    r0 = fma(-bi, xi[m], r0);
+    i0 = fma(br, xi[m], i0);
+    i0 = fma(bi, xr[m], i0);
+  }
+  ar += r0;
+  ai += i0;
+}
+
+// Returns false when a bounded wait gave up (the solve result is then invalid
+// and *P.err is set).  `phase` holds the parity bits of the two barriers and
+// is carried across calls; every thread of the CTA calls this.
+template <typename FT>
+__device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uint32_t& phase) {
+  if (*P.err) return false;
+  const int ns = S.R ? S.R->ns : S.Cf->ns;
+  const int nv = S.R ? S.R->nv : S.Cf->nv;
+  const int nstage = 2 * ns + 1;
+  const int tid = threadIdx.x;
+  // roles
+  const int nreal = S.nr * nv;
+  const int cbase = (nreal + 31) & ~31;
+  int Gc = 4;
+  while (Gc > 1 && cbase + Gc * nv > int(blockDim.x)) Gc >>= 1;
+  const bool is_r = tid < nreal;
+  const int rsys = is_r ? tid / nv : 0;
+  const int rj = is_r ? tid - rsys * nv : 0;
+  const bool is_c = S.nc > 0 && tid >= cbase && tid < cbase + Gc * nv;
+  const int cu = is_c ? tid - cbase : 0;
+  const int cj = cu / Gc, cg = cu - cj * Gc;
+  const int nv4 = 4 * nv;
+  double* ring_c_re = P.ring + S.nr * nv4;
+  double* ring_c_im = ring_c_re + nv4;
+
+  uint32_t pend = 0;  // buffers with a stage in flight (thread 0's view)
+  if (tid == 0) {
+    stage_issue<FT>(S, P, 0);
+    pend |= 1u;
+    if (nstage > 1) {
+      stage_issue<FT>(S, P, 1);
+      pend |= 2u;
+    }
+  }
+  bool ok = true;
+  for (int s = 0; s < nstage; ++s) {
+    const int b = s & 1;
+    if (mbar_wait_bounded(P.bar + b, (phase >> b) & 1u, kBulkWaitLimit)) {
+      phase ^= 1u << b;
+      pend &= ~(1u << b);
+    } else {
+      ok = false;
+      *P.err = 1;
+    }
+    ok = __all_sync(0xffffffffu, ok);  // uniform per warp before the group shuffles
+    const unsigned char* buf = P.buf[b];
+    const bool fwd = s <= ns;
+    const int i = fwd ? s : 2 * ns - s;
+    if (ok) {
+      if (is_r) {
+        const double* ring = P.ring + rsys * nv4;
+        double a = 0.0, z = 0.0;
+        if (fwd) {
+          for (int g = 0; g < 3; ++g)
+            if (i < ns && i - 3 + g >= 0)
+              col_dot(reinterpret_cast<const FT*>(buf + g * P.slot_r) + rj, ring + ((i - 3 + g) & 3) * nv, nv, a);
+          if (i >= 1) col_dot(reinterpret_cast<const FT*>(buf + 3 * P.slot_r) + rj, ring + ((i - 1) & 3) * nv, nv, z);
+          if (i < ns) P.ring[rsys * nv4 + (i & 3) * nv + rj] = S.xr[rsys][i * nv + rj] - a;
+          if (i >= 1) S.zr[rsys][(i - 1) * nv + rj] = z;
+        } else {
+          for (int g = 0; g < 3; ++g)
+            if (i + 1 + g < ns)
+              col_dot(reinterpret_cast<const FT*>(buf + g * P.slot_r) + rj, ring + ((i + 1 + g) & 3) * nv, nv, a);
+          const double x = S.zr[rsys][i * nv + rj] - a;
+          P.ring[rsys * nv4 + (i & 3) * nv + rj] = x;
+          S.xr[rsys][i * nv + rj] = x;
+        }
+      }
+      double ar = 0.0, ai = 0.0, zr = 0.0, zi = 0.0;
+      if (is_c) {
+        const unsigned char* cb = buf + 4 * P.slot_r;
+        for (int g = cg; g < 4; g += Gc) {
+          const Cx<FT>* col = reinterpret_cast<const Cx<FT>*>(cb + g * P.slot_c) + cj;
+          if (fwd) {
+            if (g < 3) {
+              if (i < ns && i - 3 + g >= 0) {
+                const int seg = ((i - 3 + g) & 3) * nv;
+                col_dot_c(col, ring_c_re + seg, ring_c_im + seg, nv, ar, ai);
+              }
+            } else if (i >= 1) {
+              const int seg = ((i - 1) & 3) * nv;
+              col_dot_c(col, ring_c_re + seg, ring_c_im + seg, nv, zr, zi);
+            }
+          } else if (g < 3 && i + 1 + g < ns) {
+            const int seg = ((i + 1 + g) & 3) * nv;
+            col_dot_c(col, ring_c_re + seg, ring_c_im + seg, nv, ar, ai);
+          }
+        }
+      }
+      // group reduction over the Gc lanes of a complex row (uniform in the warp)
+      for (int o = Gc >> 1; o > 0; o >>= 1) {
+        ar += __shfl_down_sync(0xffffffffu, ar, o, Gc);
+        ai += __shfl_down_sync(0xffffffffu, ai, o, Gc);
+        zr += __shfl_down_sync(0xffffffffu, zr, o, Gc);
+        zi += __shfl_down_sync(0xffffffffu, zi, o, Gc);
+      }
+      if (is_c && cg == 0) {
+        if (fwd) {
+          if (i < ns) {
+            ring_c_re[(i & 3) * nv + cj] = S.xc_re[i * nv + cj] - ar;
+            ring_c_im[(i & 3) * nv + cj] = S.xc_im[i * nv + cj] - ai;
+          }
+          if (i >= 1) {
+            S.zc_re[(i - 1) * nv + cj] = zr;
+            S.zc_im[(i - 1) * nv + cj] = zi;
+          }
+        } else {
+          const double xr = S.zc_re[i * nv + cj] - ar, xi = S.zc_im[i * nv + cj] - ai;
+          ring_c_re[(i & 3) * nv + cj] = xr;
+          ring_c_im[(i & 3) * nv + cj] = xi;
+          S.xc_re[i * nv + cj] = xr;
+          S.xc_im[i * nv + cj] = xi;
+        }
+      }
+    }
+    __syncthreads();
+    if (*P.err) {
+      ok = false;
+      break;
+    }
+    if (tid == 0 && s + 2 < nstage) {
+      stage_issue<FT>(S, P, s + 2);
+      pend |= 1u << b;
+    }
+  }
+  if (!ok && tid == 0) {
+    // let copies still in flight land (bounded) before the buffers are reused
+    for (int b = 0; b < 2; ++b)
+      if ((pend >> b) & 1u) mbar_wait_bounded(P.bar + b, (phase >> b) & 1u, kBulkWaitLimit);
+  }
+  __syncthreads();
+  return ok;
 }
 
 }  // namespace fpe

@@ -248,8 +248,8 @@ static int plan_layout(FpePlan* P, int esz) {
     const int ns_cap = std::min(d.cap_dof_s, FPE_MAX_NDOF_S);
     const int ebytes = cplx ? 2 * esz : esz;  // the complex factor needs the larger scratch
     size_t base = sizeof(fpe::RadauSmem) + size_t(4 * ns_cap * 7 + 5 * nv * 7) * 8 + 64;
-    size_t sm = base + size_t(fpe::blu_smem_elems_v2(nv)) * esz +
-                (cplx ? size_t(fpe::blu_smem_elems_v2(nv)) * 2 * esz + 16 : 0);
+    size_t sm = base + size_t(fpe_fac_scratch_elems(nv)) * esz +
+                (cplx ? size_t(fpe_fac_scratch_elems(nv)) * 2 * esz + 16 : 0);
     (void)ebytes;
     smem_base_max = std::max(smem_base_max, base);
     smem_max = std::max(smem_max, sm);
@@ -391,6 +391,32 @@ static FpePlan* plan_build(const FpeContract* c, int n, const Opts& o, bool save
     } else {
       p.solve_a = int(P->descs.size());
       P->descs.push_back(make_desc(p, ot, p.barrier, o));
+    }
+  }
+  // Launch the solves longest first.  One CTA runs one solve to completion and
+  // the block scheduler hands out CTAs in index order, so ordering by the
+  // estimated cost (stage factorization ~ ns nv^3, step count growing slowly
+  // with T) is longest-processing-time list scheduling over the SMs.
+  if (P->descs.size() > 1) {
+    const size_t n = P->descs.size();
+    std::vector<double> cost(n);
+    for (size_t s = 0; s < n; ++s) {
+      const FpeSolveDesc& d = P->descs[s];
+      const double ns = d.cap_dof_s, nv = d.cap_dof_v;
+      cost[s] = ns * nv * nv * (nv + 8.0) * (1.0 + 0.2 * std::log1p(d.T / 0.1));
+    }
+    std::vector<int> perm(n), pos(n);
+    for (size_t s = 0; s < n; ++s) perm[s] = int(s);
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<FpeSolveDesc> sorted(n);
+    for (size_t k = 0; k < n; ++k) {
+      sorted[k] = P->descs[perm[k]];
+      pos[perm[k]] = int(k);
+    }
+    P->descs.swap(sorted);
+    for (auto& p : P->pricings) {
+      if (p.solve_a >= 0) p.solve_a = pos[p.solve_a];
+      if (p.solve_b >= 0) p.solve_b = pos[p.solve_b];
     }
   }
   // each solve prices into its own slot range
@@ -739,6 +765,8 @@ int32_t fpe_plan_stats(FpePlan* P, int64_t* out) {
     out[15] += in[FPE_INFO_T_SOLVE];
     out[16] += in[FPE_INFO_T_KRON];
     out[17] += in[FPE_INFO_T_TOTAL];
+    out[18] += in[FPE_INFO_T_FGJ];
+    out[19] += in[FPE_INFO_T_FGEMM];
   }
   return 0;
 }
@@ -1132,8 +1160,8 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
     const int ns_cap = std::min(d[k].cap_dof_s, FPE_MAX_NDOF_S);
     const size_t b = sizeof(fpe::RadauSmem) + size_t(4 * ns_cap * 7 + 5 * nv * 7) * 8 + 64;
     smem_base = std::max(smem_base, b);
-    smem_max = std::max(smem_max, b + size_t(fpe::blu_smem_elems_v2(nv)) * esz +
-                                      (o.complex_mode ? size_t(fpe::blu_smem_elems_v2(nv)) * 2 * esz + 16 : 0));
+    smem_max = std::max(smem_max, b + size_t(fpe_fac_scratch_elems(nv)) * esz +
+                                      (o.complex_mode ? size_t(fpe_fac_scratch_elems(nv)) * 2 * esz + 16 : 0));
     const size_t nsd = d[k].cap_dof_s, nvd = d[k].cap_dof_v;
     ic = std::max(ic, (nsd * nsd + nvd * nvd + 7 * nsd * nvd) * sizeof(double));
   }

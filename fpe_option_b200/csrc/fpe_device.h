@@ -21,6 +21,7 @@ enum FpeStatus : int32_t {
   FPE_ERR_MAX_STEPS = 4,     // radau.mojo:257-263
   FPE_ERR_STEP_UNDERFLOW = 5,// radau.mojo:274-281, :458-464
   FPE_ERR_NONFINITE = 6,
+  FPE_ERR_TIMEOUT = 7,       // a bounded wait on an asynchronous copy gave up
 };
 
 // Per-solve counters written by the kernels (int32 arena, FPE_INFO_* slots).
@@ -32,6 +33,8 @@ enum FpeInfo {
   FPE_INFO_ADMM, FPE_INFO_PASS_REAL, FPE_INFO_NSAVED, FPE_INFO_PASS_CPLX,
   // SM clock cycles / 1024 spent in the Radau kernel phases (thread 0's view)
   FPE_INFO_T_FACTOR, FPE_INFO_T_SOLVE, FPE_INFO_T_KRON, FPE_INFO_T_TOTAL,
+  FPE_INFO_T_FGJ,    // inside T_FACTOR: pivot-block Gauss-Jordan (kilocycles)
+  FPE_INFO_T_FGEMM,  // inside T_FACTOR: L / W products and Schur updates (kilocycles)
   FPE_INFO_COUNT = 24
 };
 
@@ -97,6 +100,22 @@ struct FpeILayout {
 #define FPE_HD inline
 #endif
 
+// Stage-factorization scratch of one system, in elements: the pivot block's
+// Gauss-Jordan array nv x (nv + 1), then blocks padded to nvp = nv rounded up
+// to 4 (row-major nvp x nvp, transposed nvp x (nvp + 4)): P^-1 both ways, three
+// transposed E and L blocks, three U blocks, and the pivot bookkeeping (with
+// room to spare).
+FPE_HD int fpe_fac_nvp(int nv) { return (nv + 3) & ~3; }
+// Element stride between the nv x nv blocks of a stored stage factor: nv^2
+// rounded up to 4, so every block starts and ends on a 16-byte boundary and
+// moves with one bulk copy.
+FPE_HD int fpe_block_stride(int nv) { return (nv * nv + 3) & ~3; }
+FPE_HD int fpe_fac_scratch_elems(int nv) {
+  const int p = fpe_fac_nvp(nv), t = p + 4;
+  const int aug = (nv * (nv + 1) + 3) & ~3;
+  return aug + p * p + p * t + 3 * p * t + 3 * p * t + 3 * p * p + 3 * p + (3 * p + 4);
+}
+
 FPE_HD FpeDLayout fpe_dlayout(const FpeSolveDesc& d) {
   FpeDLayout L;
   int64_t o = 0;
@@ -132,9 +151,9 @@ FPE_HD FpeDLayout fpe_dlayout(const FpeSolveDesc& d) {
   L.q0 = take(N);
   L.y = take(N);
   L.qT = take(N);
-  // FP64 worst case of the real + complex factor scratch:
-  // 3 x (nv (2nv+1) + 10 nv^2 + 6 nv + 16) doubles + alignment
-  L.fsc = take(40 * int64_t(d.cap_dof_v) * d.cap_dof_v + 64 * int64_t(d.cap_dof_v) + 128);
+  // FP64 worst case of the real + complex factor scratch (elements of 8 and
+  // 16 bytes) plus the 16-byte alignment of the complex part
+  L.fsc = take(3 * int64_t(fpe_fac_scratch_elems(d.cap_dof_v)) + 8);
   int64_t dense = int64_t(d.cap_dof_s) * d.cap_dof_s + int64_t(d.cap_dof_v) * d.cap_dof_v;
   L.work = take(int64_t(FPE_WORK_VECS) * N + 4 * dense + 256);
   L.total = o;
@@ -162,7 +181,7 @@ FPE_HD FpeILayout fpe_ilayout(const FpeSolveDesc& d) {
 // rows x 7 blocks of nv x nv) of element size esz, plus the same for the
 // complex system when requested (2 * esz per entry).
 FPE_HD int64_t fpe_factor_bytes(const FpeSolveDesc& d, int esz, int with_complex) {
-  int64_t blocks = int64_t(d.cap_dof_s) * 7 * d.cap_dof_v * d.cap_dof_v;
+  int64_t blocks = int64_t(d.cap_dof_s) * 7 * fpe_block_stride(d.cap_dof_v);
   int64_t b = blocks * esz;
   if (with_complex) b += blocks * 2 * esz;
   return (b + 255) & ~int64_t(255);

@@ -47,7 +47,8 @@ enum RadauVec {
   RV_CERR, RV_MCONT, RV_RERR, RV_ERR, RV_YT, RV_RES, RV_RES2, RV_RES3, RV_WR, RV_WI,
   RV_Z0, RV_ZA, RV_ZB, RV_ZC,  // block-solve z scratch (2 real + complex re/im)
   RV_VR = 37, RV_VI = RV_VR + FPE_GMRES_M + 1, RV_TMP = RV_VI + FPE_GMRES_M + 1,  // 15 temps
-  RV_COUNT = RV_TMP + 15
+  RV_GB0 = RV_TMP + 15, RV_GB1, RV_GR0, RV_GR1,  // refined GMRES preconditioner applies
+  RV_COUNT = RV_GR1 + 1
 };
 static_assert(RV_COUNT <= FPE_WORK_VECS, "work area too small");
 
@@ -106,6 +107,8 @@ __device__ void kron_apply(const RadauCtx& C, const KronTerm* terms, int nt, con
 }
 
 struct RadauSmem {
+  unsigned long long pipe_bar[2];  // stage-buffer barriers of the staged block solve
+  int pipe_err, pipe_pad;
   double red[32 * 8];
   double H[(FPE_GMRES_M + 1) * FPE_GMRES_M];
   double gcs[FPE_GMRES_M + 1], gsn[FPE_GMRES_M + 1], gs[FPE_GMRES_M + 1], gy[FPE_GMRES_M + 1];
@@ -160,7 +163,7 @@ __device__ void apply_E2(const RadauCtx& C, const KronTerm* Edt, const KronTerm*
 }
 
 template <typename FT>
-__global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
+__global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RadauSmem& S = *reinterpret_cast<RadauSmem*>(smem_raw);
   const FpeSolveDesc d = A.descs[blockIdx.x];
@@ -181,13 +184,36 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
                                              ~uintptr_t(15));
   for (int e = threadIdx.x; e < 4 * ns * 7; e += blockDim.x) fs[e] = D[DL.op_s + e];
   for (int e = threadIdx.x; e < 5 * nv * 7; e += blockDim.x) fv[e] = D[DL.op_v + e];
+  if (threadIdx.x == 0) {
+    mbar_init(&S.pipe_bar[0], 1);
+    mbar_init(&S.pipe_bar[1], 1);
+    S.pipe_err = 0;
+    mbar_init_fence();
+  }
   __syncthreads();
   RadauCtx C{ns, nv, N, D + DL.work};
   const OpFactors O{ns, nv, fs, fs + ns * 7, fs + 2 * ns * 7, fs + 3 * ns * 7,
                     fv, fv + nv * 7, fv + 2 * nv * 7, fv + 3 * nv * 7, fv + 4 * nv * 7};
   FT* fbase = reinterpret_cast<FT*>(A.farena + d.off_f);
-  const BlockLU<FT> LR{fbase, ns, nv};
-  const BlockLU<Cx<FT>> LC{reinterpret_cast<Cx<FT>*>(fbase + size_t(ns) * 7 * nv * nv), ns, nv};
+  const int bs = fpe_block_stride(nv);
+  const BlockLU<FT> LR{fbase, ns, nv, bs};
+  const BlockLU<Cx<FT>> LC{reinterpret_cast<Cx<FT>*>(fbase + size_t(ns) * 7 * bs), ns, nv, bs};
+  // Staged sweeps when the stage buffers fit in the (shared) factorization
+  // scratch, which is idle while the sweeps run.
+  const int esz = int(sizeof(FT));
+  const long long fac_bytes = A.fac_global ? 0
+                              : (long long)fpe_fac_scratch_elems(nv) * esz *
+                                        (direct ? 3 : 1) + (direct ? 16 : 0);
+  const bool staged = fac_bytes >= stage_total_bytes(nv, esz, direct);
+  SolveStage SP;
+  SP.slot_r = stage_slot_bytes(nv, esz);
+  SP.slot_c = stage_slot_bytes(nv, 2 * esz);
+  SP.buf[0] = reinterpret_cast<unsigned char*>(sbig);
+  SP.buf[1] = SP.buf[0] + 4 * SP.slot_r + (direct ? 4 * SP.slot_c : 0);
+  SP.ring = reinterpret_cast<double*>(SP.buf[1] + 4 * SP.slot_r + (direct ? 4 * SP.slot_c : 0));
+  SP.bar = S.pipe_bar;
+  SP.err = &S.pipe_err;
+  uint32_t pipe_phase = 0;
   const KronTerm Kt[4] = {{O.Ss, O.B1, 1.0}, {O.Ts, O.B2, 1.0}, {O.As, O.B3, 1.0}, {O.St, O.B4, 1.0}};
   const KronTerm Mt[1] = {{O.As, O.Av, 1.0}};
   using namespace rc;
@@ -212,6 +238,7 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
   // phase timers (SM clock cycles, thread 0 reports)
   const long long t_kernel0 = clock64();
   long long t_factor = 0, t_solve = 0, t_kron = 0;
+  long long t_fsub[2] = {0, 0};  // factorization: Gauss-Jordan, GEMMs
 #define KRON(...)                          \
   do {                                     \
     const long long t_k0 = clock64();      \
@@ -237,16 +264,24 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
     Sv.zc_re = vslot(C, RV_ZB);
     Sv.zc_im = vslot(C, RV_ZC);
     Sv.nc = nc;
-    blu_solve<FT>(Sv);
+    if (staged) {
+      blu_solve_staged<FT>(Sv, SP, pipe_phase);
+    } else {
+      blu_solve<FT>(Sv);
+    }
     t_solve += clock64() - t_s0;
   };
   KronTerm E1t[5], Edt[5];
+  // FP64 refinement sweeps per stage solve.  In the GMRES path (reference
+  // parity) FP32 factors get at least one, so that the simplified-Newton and
+  // GMRES(10) iterates follow those of an FP64 factor.
+  const int nref = (sizeof(FT) == 4 && !direct && A.nref < 1) ? 1 : A.nref;
   // x = E1^-1 b (+ nref FP64 refinement sweeps)
   auto solve_real = [&](double* x, const double* b) {
     for (int e = threadIdx.x; e < N; e += blockDim.x) x[e] = b[e];
     __syncthreads();
     solve_set(x, nullptr, 1, nullptr, nullptr, 0);
-    for (int it = 0; it < A.nref; ++it) {
+    for (int it = 0; it < nref; ++it) {
       const double* xc[1] = {x};
       double* rs[1] = {res};
       kron_apply(C, E1t, 5, xc, rs, 1);
@@ -254,6 +289,38 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
       __syncthreads();
       solve_set(res, nullptr, 1, nullptr, nullptr, 0);
       for (int e = threadIdx.x; e < N; e += blockDim.x) x[e] += res[e];
+      __syncthreads();
+    }
+  };
+
+  // GMRES preconditioner apply x_k = E1^-1 x_k (k = 0, 1), refined like the
+  // real stage solves.
+  const int nref_g = nref;
+  double *gb0 = vslot(C, RV_GB0), *gb1 = vslot(C, RV_GB1);
+  double *gr0 = vslot(C, RV_GR0), *gr1 = vslot(C, RV_GR1);
+  auto solve_real2 = [&](double* x0, double* x1) {
+    if (nref_g > 0) {
+      for (int e = threadIdx.x; e < N; e += blockDim.x) {
+        gb0[e] = x0[e];
+        gb1[e] = x1[e];
+      }
+      __syncthreads();
+    }
+    solve_set(x0, x1, 2, nullptr, nullptr, 0);
+    for (int it = 0; it < nref_g; ++it) {
+      const double* xc[2] = {x0, x1};
+      double* rs[2] = {gr0, gr1};
+      KRON(C, E1t, 5, xc, rs, 2);
+      for (int e = threadIdx.x; e < N; e += blockDim.x) {
+        gr0[e] = gb0[e] - gr0[e];
+        gr1[e] = gb1[e] - gr1[e];
+      }
+      __syncthreads();
+      solve_set(gr0, gr1, 2, nullptr, nullptr, 0);
+      for (int e = threadIdx.x; e < N; e += blockDim.x) {
+        x0[e] += gr0[e];
+        x1[e] += gr1[e];
+      }
       __syncthreads();
     }
   };
@@ -293,6 +360,10 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
 
   long n_loop = 0;
   while (posneg * (t1 - t) > uround * fmax(fabs(t), fabs(t1))) {
+    if (S.pipe_err) {  // a staged sweep's bounded wait gave up: stop this solve
+      status = FPE_ERR_TIMEOUT;
+      break;
+    }
     if (n_steps > 100000 || ++n_loop > 400000) {
       status = FPE_ERR_MAX_STEPS;
       break;
@@ -315,8 +386,8 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
       if (direct) blu_assemble<Cx<FT>>(O, LC, ALPH, BETA, h);
       FT* scr_r = reinterpret_cast<FT*>(sbig);
       Cx<FT>* scr_c = reinterpret_cast<Cx<FT>*>(
-          (reinterpret_cast<uintptr_t>(scr_r + blu_smem_elems_v2(nv)) + 15) & ~uintptr_t(15));
-      if (!blu_factor_pair<FT>(LR, direct ? &LC : nullptr, scr_r, scr_c)) status = FPE_ERR_SINGULAR;
+          (reinterpret_cast<uintptr_t>(scr_r + fpe_fac_scratch_elems(nv)) + 15) & ~uintptr_t(15));
+      if (!blu_factor_pair<FT>(LR, direct ? &LC : nullptr, scr_r, scr_c, t_fsub)) status = FPE_ERR_SINGULAR;
       t_factor += clock64() - t_f0;
       ++n_lu;
       h_lu = h;
@@ -387,7 +458,7 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
         }
         __syncthreads();
         solve_set(dF1, nullptr, 1, dF2, dF3, 1);
-        for (int it = 0; it < A.nref; ++it) {
+        for (int it = 0; it < nref; ++it) {
           const double* xc[1] = {dF1};
           double* rs[1] = {res};
           KRON(C, E1t, 5, xc, rs, 1);
@@ -416,7 +487,7 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
           Vi0[e] = rim[e];
         }
         __syncthreads();
-        solve_set(Vr0, Vi0, 2, nullptr, nullptr, 0);
+        solve_real2(Vr0, Vi0);
         double part = 0.0;
         for (int e = threadIdx.x; e < N; e += blockDim.x) part += Vr0[e] * Vr0[e] + Vi0[e] * Vi0[e];
         const double beta = sqrt(block_sum1(part, S.red));
@@ -443,7 +514,7 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
             const double* Vrj = vslot(C, RV_VR + j);
             const double* Vij = vslot(C, RV_VI + j);
             apply_E2(C, Edt, Mt, BETA, Vrj, Vij, wr, wi, res, res2);
-            solve_set(wr, wi, 2, nullptr, nullptr, 0);
+            solve_real2(wr, wi);
             ++n_gmres;
             for (int k = 0; k <= j; ++k) {  // modified Gram-Schmidt, real inner product
               const double* Vrk = vslot(C, RV_VR + k);
@@ -676,6 +747,8 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_radau(RadauKernelArgs<FT> A) {
     info[FPE_INFO_T_SOLVE] = int(t_solve >> 10);
     info[FPE_INFO_T_KRON] = int(t_kron >> 10);
     info[FPE_INFO_T_TOTAL] = int((clock64() - t_kernel0) >> 10);
+    info[FPE_INFO_T_FGJ] = int(t_fsub[0] >> 10);
+    info[FPE_INFO_T_FGEMM] = int(t_fsub[1] >> 10);
   }
 }
 

@@ -174,6 +174,7 @@ typedef struct FpeBatchOptions {
 #define FPE_STATUS_MAX_STEPS 4
 #define FPE_STATUS_STEP_UNDERFLOW 5
 #define FPE_STATUS_NONFINITE 6
+#define FPE_STATUS_TIMEOUT 7  /* a bounded device-side wait gave up (no reference counterpart) */
 #define FPE_STATUS_INVALID 16
 
 /** A prepared batch: descriptors and strikes resident on the device.
@@ -198,7 +199,9 @@ extern int32_t fpe_plan_results(FpePlan* plan, double* prices, double* delta, do
  *  [9] total dofs, [10] sweeps over real factors, [11] sweeps over complex
  *  factors, [12] algorithmic stage-factor bytes (written + read), [13] worst
  *  status, [14]-[17] SM kilo-cycles summed over solves spent in the Radau
- *  kernel's factorizations, block solves, Kronecker products and in total. */
+ *  kernel's factorizations, block solves, Kronecker products and in total,
+ *  [18]-[19] the parts of [14] spent in the pivot-block Gauss-Jordan
+ *  eliminations and in the block products (L, W and Schur updates). */
 extern int32_t fpe_plan_stats(FpePlan* plan, int64_t* out);
 /** Run the pipeline once with a CUDA event around each of its five kernels
  *  (setup, galerkin, ic, radau, payoff); ms[5] receives the durations. */
