@@ -264,10 +264,7 @@ static int plan_layout(FpePlan* P, int esz) {
   P->fac_global = smem_max > optin ? 1 : 0;
   // ADMM iterates of the IC projection in shared memory when they fit
   size_t ic = 0;
-  for (auto& d : P->descs) {
-    const size_t ns = d.cap_dof_s, nv = d.cap_dof_v;
-    ic = std::max(ic, (ns * ns + nv * nv + 7 * ns * nv) * sizeof(double));
-  }
+  for (auto& d : P->descs) ic = std::max(ic, fpe_ic_admm_bytes(d.cap_dof_s, d.cap_dof_v));
   const size_t ic_lim = optin - sizeof(fpe::IcSmem) - 1024;
   P->ic_smem = ic <= ic_lim ? ic : 0;
   P->radau_smem = P->fac_global ? smem_base_max : smem_max;
@@ -1162,8 +1159,7 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
     smem_base = std::max(smem_base, b);
     smem_max = std::max(smem_max, b + size_t(fpe_fac_scratch_elems(nv)) * esz +
                                       (o.complex_mode ? size_t(fpe_fac_scratch_elems(nv)) * 2 * esz + 16 : 0));
-    const size_t nsd = d[k].cap_dof_s, nvd = d[k].cap_dof_v;
-    ic = std::max(ic, (nsd * nsd + nvd * nvd + 7 * nsd * nvd) * sizeof(double));
+    ic = std::max(ic, fpe_ic_admm_bytes(d[k].cap_dof_s, d[k].cap_dof_v));
   }
   const size_t off_d = off;
   off = up(off + size_t(od) * sizeof(double));

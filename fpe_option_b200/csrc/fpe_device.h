@@ -116,6 +116,15 @@ FPE_HD int fpe_fac_scratch_elems(int nv) {
   return aug + p * p + p * t + 3 * p * t + 3 * p * t + 3 * p * p + 3 * p + (3 * p + 4);
 }
 
+// Shared memory of the IC projection's ADMM (bytes): eigenvector matrices
+// Vs (nds^2), Vv and Vv^T (ndv^2 each), the five iterates, lam and q (N each),
+// every section rounded to an even number of doubles.
+FPE_HD size_t fpe_ic_admm_bytes(int nds, int ndv) {
+  auto ev = [](size_t n) { return (n + 1) & ~size_t(1); };
+  const size_t N = size_t(nds) * ndv;
+  return (ev(size_t(nds) * nds) + 2 * ev(size_t(ndv) * ndv) + 7 * ev(N)) * sizeof(double);
+}
+
 FPE_HD FpeDLayout fpe_dlayout(const FpeSolveDesc& d) {
   FpeDLayout L;
   int64_t o = 0;

@@ -52,6 +52,63 @@ __device__ void cta_gemm2(int m, int n, int k, const double* __restrict__ A, int
   }
 }
 
+// C[m x n] = op(A) B (.* scale) with a 2 x 4 register tile per thread:
+// element (r, p) of op(A) at A[r*ar + p*ac]; B row-major with row stride ldb.
+// When vec is set (ldb even, B 16-byte aligned) a tile row of B is two
+// 16-byte loads.  Consecutive threads take consecutive column tiles, so a
+// warp reads contiguous rows of B.
+__device__ void cta_gemm24(int m, int n, int k, const double* __restrict__ A, int ar, int ac,
+                           const double* __restrict__ B, int ldb, double* __restrict__ C, int ldc,
+                           const double* __restrict__ scale, bool vec) {
+  const int mt = (m + 1) / 2, nt = (n + 3) / 4;
+  for (int t = threadIdx.x; t < mt * nt; t += blockDim.x) {
+    const int ti = t / nt, tj = t - ti * nt;
+    const int r0 = 2 * ti, r1 = r0 + 1 < m ? r0 + 1 : r0;
+    const int c0 = 4 * tj;
+    const double* a0 = A + r0 * ar;
+    const double* a1 = A + r1 * ar;
+    double acc0[4] = {0.0, 0.0, 0.0, 0.0}, acc1[4] = {0.0, 0.0, 0.0, 0.0};
+    if (vec && c0 + 3 < n) {
+#pragma unroll 4
+      for (int p = 0; p < k; ++p) {
+        const double x0 = a0[p * ac], x1 = a1[p * ac];
+        const double2 b01 = *reinterpret_cast<const double2*>(B + p * ldb + c0);
+        const double2 b23 = *reinterpret_cast<const double2*>(B + p * ldb + c0 + 2);
+        acc0[0] = fma(x0, b01.x, acc0[0]);
+        acc0[1] = fma(x0, b01.y, acc0[1]);
+        acc0[2] = fma(x0, b23.x, acc0[2]);
+        acc0[3] = fma(x0, b23.y, acc0[3]);
+        acc1[0] = fma(x1, b01.x, acc1[0]);
+        acc1[1] = fma(x1, b01.y, acc1[1]);
+        acc1[2] = fma(x1, b23.x, acc1[2]);
+        acc1[3] = fma(x1, b23.y, acc1[3]);
+      }
+    } else {
+      for (int p = 0; p < k; ++p) {
+        const double x0 = a0[p * ac], x1 = a1[p * ac];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const double b = c0 + j < n ? B[p * ldb + c0 + j] : 0.0;
+          acc0[j] = fma(x0, b, acc0[j]);
+          acc1[j] = fma(x1, b, acc1[j]);
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + j;
+      if (c >= n) break;
+      double v0 = acc0[j], v1 = acc1[j];
+      if (scale) {
+        v0 *= scale[r0 * ldc + c];
+        v1 *= scale[r1 * ldc + c];
+      }
+      C[r0 * ldc + c] = v0;
+      if (r1 != r0) C[r1 * ldc + c] = v1;
+    }
+  }
+}
+
 // Cyclic Jacobi eigendecomposition of the symmetric n x n matrix A (row-major,
 // destroyed; eigenvalues left on its diagonal), eigenvectors in the columns
 // of V.  Round-robin ordering: n/2 disjoint rotations per round.
@@ -189,7 +246,7 @@ struct IcSmem {
   double cs[4 * 96];
 };
 
-__global__ void __launch_bounds__(FPE_BLOCK) k_ic(const FpeSolveDesc* __restrict__ descs,
+__global__ void __launch_bounds__(FPE_BLOCK, 1) k_ic(const FpeSolveDesc* __restrict__ descs,
                                                   double* __restrict__ darena,
                                                   int32_t* __restrict__ iarena, int32_t* __restrict__ infos,
                                                   size_t dyn_bytes) {
@@ -338,22 +395,26 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_ic(const FpeSolveDesc* __restrict
   __syncthreads();
 
   // ---- ADMM (osqp.mojo:93-157) ------------------------------------------
-  // Shared-memory resident when it fits (eigenvectors + five iterates + lam, q).
-  const size_t need = (size_t(nds) * nds + size_t(ndv) * ndv + 7 * size_t(N)) * sizeof(double);
+  // Shared-memory resident when it fits: eigenvectors Vs, Vv and Vv^T, the
+  // five iterates, lam and q, each section at an even (16-byte) offset.
+  const size_t need = fpe_ic_admm_bytes(nds, ndv);
   double* sVs = Vs;
   double* sVv = Vv;
+  double* sVvT = vec + 8 * size_t(N);  // global fallback: after the iterates (work area)
   double *sx = x, *sz = z, *su = u, *sq = q, *srhs = rhs, *st1 = t1, *slam = lam;
+  auto ev = [](int n) { return (n + 1) & ~1; };
   if (need <= dyn_bytes) {
     double* sm = reinterpret_cast<double*>(ic_dyn);
     sVs = sm;
-    sVv = sVs + nds * nds;
-    sx = sVv + ndv * ndv;
-    sz = sx + N;
-    su = sz + N;
-    sq = su + N;
-    srhs = sq + N;
-    st1 = srhs + N;
-    slam = st1 + N;
+    sVv = sVs + ev(nds * nds);
+    sVvT = sVv + ev(ndv * ndv);
+    sx = sVvT + ev(ndv * ndv);
+    sz = sx + ev(N);
+    su = sz + ev(N);
+    sq = su + ev(N);
+    srhs = sq + ev(N);
+    st1 = srhs + ev(N);
+    slam = st1 + ev(N);
     for (int e = threadIdx.x; e < nds * nds; e += blockDim.x) sVs[e] = Vs[e];
     for (int e = threadIdx.x; e < ndv * ndv; e += blockDim.x) sVv[e] = Vv[e];
     for (int e = threadIdx.x; e < N; e += blockDim.x) {
@@ -363,21 +424,29 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_ic(const FpeSolveDesc* __restrict
       sq[e] = q[e];
       slam[e] = lam[e];
     }
-    __syncthreads();
   }
+  for (int e = threadIdx.x; e < ndv * ndv; e += blockDim.x) {
+    const int r = e / ndv, c = e - r * ndv;
+    sVvT[c * ndv + r] = Vv[e];
+  }
+  __syncthreads();
+  // 16-byte loads of the right operands need an even row stride and aligned rows
+  const bool vec_v = (ndv & 1) == 0 && ((reinterpret_cast<uintptr_t>(sVv) | reinterpret_cast<uintptr_t>(sVvT) |
+                                        reinterpret_cast<uintptr_t>(srhs) | reinterpret_cast<uintptr_t>(sx) |
+                                        reinterpret_cast<uintptr_t>(st1)) & 15) == 0;
   int it = 0;
   for (it = 0; it < 50000; ++it) {
     for (int e = threadIdx.x; e < N; e += blockDim.x)
       srhs[e] = sq[e] + rho * (sz[e] - su[e]) + sigma * sx[e];
     __syncthreads();
     // x = (Vs (x) Vv) diag(lam) (Vs (x) Vv)^T rhs
-    cta_gemm2(nds, ndv, nds, sVs, 1, nds, srhs, ndv, 1, st1, ndv, nullptr);  // Vs^T R
+    cta_gemm24(nds, ndv, nds, sVs, 1, nds, srhs, ndv, st1, ndv, nullptr, vec_v);  // Vs^T R
     __syncthreads();
-    cta_gemm2(nds, ndv, ndv, st1, ndv, 1, sVv, ndv, 1, sx, ndv, slam);  // ((Vs^T R) Vv) .* lam
+    cta_gemm24(nds, ndv, ndv, st1, ndv, 1, sVv, ndv, sx, ndv, slam, vec_v);  // ((Vs^T R) Vv) .* lam
     __syncthreads();
-    cta_gemm2(nds, ndv, nds, sVs, nds, 1, sx, ndv, 1, st1, ndv, nullptr);  // Vs X
+    cta_gemm24(nds, ndv, nds, sVs, nds, 1, sx, ndv, st1, ndv, nullptr, vec_v);  // Vs X
     __syncthreads();
-    cta_gemm2(nds, ndv, ndv, st1, ndv, 1, sVv, 1, ndv, sx, ndv, nullptr);  // (Vs X) Vv^T
+    cta_gemm24(nds, ndv, ndv, st1, ndv, 1, sVvT, ndv, sx, ndv, nullptr, vec_v);  // (Vs X) Vv^T
     __syncthreads();
     double nr[5] = {0, 0, 0, 0, 0};
     for (int e = threadIdx.x; e < N; e += blockDim.x) {
