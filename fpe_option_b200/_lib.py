@@ -1,4 +1,5 @@
-"""ctypes binding of ``libfpe_engine.so`` (the C ABI in include/fpe_engine.h).
+"""ctypes binding of ``libfpe_engine.so`` (the C ABI in include/fpe_engine.h and
+include/fpe_surrogate.h).
 
 The library is built in-tree by :func:`fpe_option_b200.build.build_library`.
 There is no CPU fallback: loading fails loudly when the shared object is
@@ -56,7 +57,7 @@ class FpeBatchOptions(C.Structure):
                 ("radau_constants", i32)]
 
 
-# Every symbol declared in include/fpe_engine.h.
+# Every symbol declared in include/*.h.
 EXPORTED = [
     "fpe_compute_create", "fpe_compute_destroy", "fpe_compute_knots", "fpe_compute_grid_points",
     "fpe_compute_initial_condition", "fpe_compute_solve", "fpe_compute_pdf", "fpe_compute_price",
@@ -66,6 +67,10 @@ EXPORTED = [
     "fpe_plan_stats", "fpe_plan_sizes", "fpe_plan_destroy", "fpe_price_batch",
     "fpe_compute_create_ex", "fpe_compute_basis_csr", "fpe_device_available",
     "fpe_plan_kernel_times", "fpe_price_noalloc",
+    # include/fpe_surrogate.h
+    "fpe_mlp_create", "fpe_mlp_destroy", "fpe_mlp_layout", "fpe_mlp_get_params",
+    "fpe_mlp_set_params", "fpe_mlp_forward", "fpe_mlp_train_step", "fpe_mlp_gradient",
+    "fpe_gemm_bf16",
 ]
 
 _lib = None
@@ -122,6 +127,24 @@ def load():
     L.fpe_compute_basis_csr.argtypes = [cp, i32, ip, ip, ip, ip, dp]
     L.fpe_device_available.restype = i32
     L.fpe_device_available.argtypes = []
+    fp = C.POINTER(C.c_float)
+    L.fpe_mlp_create.restype = vp
+    L.fpe_mlp_create.argtypes = [i32, i32, i32, i32, C.c_uint64]
+    L.fpe_mlp_destroy.argtypes = [vp]
+    L.fpe_mlp_layout.restype = i64
+    L.fpe_mlp_layout.argtypes = [vp, ip]
+    L.fpe_mlp_get_params.restype = i32
+    L.fpe_mlp_get_params.argtypes = [vp, fp, i64]
+    L.fpe_mlp_set_params.restype = i32
+    L.fpe_mlp_set_params.argtypes = [vp, fp, i64]
+    L.fpe_mlp_forward.restype = i32
+    L.fpe_mlp_forward.argtypes = [vp, vp, i32, vp, vp]
+    L.fpe_mlp_train_step.restype = i32
+    L.fpe_mlp_train_step.argtypes = [vp, vp, vp, vp, i32, C.c_float, vp, vp]
+    L.fpe_mlp_gradient.restype = i32
+    L.fpe_mlp_gradient.argtypes = [vp, vp, vp, vp, i32, fp, fp]
+    L.fpe_gemm_bf16.restype = i32
+    L.fpe_gemm_bf16.argtypes = [vp, i32, vp, i32, i32, i32, i32, vp, i32, vp, i32, vp]
     L.fpe_price_noalloc.restype = i32
     L.fpe_price_noalloc.argtypes = [C.POINTER(FpeContract), C.POINTER(FpeBatchOptions), dp, ip, vp]
     _lib = L

@@ -5,7 +5,7 @@ import os
 import subprocess
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCES = [os.path.join(_HERE, "csrc", "engine.cu")]
+SOURCES = [os.path.join(_HERE, "csrc", "engine.cu"), os.path.join(_HERE, "csrc", "mlp.cu")]
 DEPS = [os.path.join(_HERE, "csrc", f) for f in os.listdir(os.path.join(_HERE, "csrc"))]
 OUT = os.path.join(_HERE, "libfpe_engine.so")
 NVCC_FLAGS = [
@@ -19,8 +19,9 @@ def _stale() -> bool:
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    inc = os.path.join(os.path.dirname(_HERE), "include", "fpe_engine.h")
-    return any(os.path.getmtime(p) > t for p in DEPS + [inc] if os.path.exists(p))
+    inc_dir = os.path.join(os.path.dirname(_HERE), "include")
+    incs = [os.path.join(inc_dir, f) for f in os.listdir(inc_dir)] if os.path.isdir(inc_dir) else []
+    return any(os.path.getmtime(p) > t for p in DEPS + incs if os.path.exists(p))
 
 
 def build_library(force: bool = False, verbose: bool = False) -> str:

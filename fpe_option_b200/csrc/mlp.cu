@@ -1,0 +1,792 @@
+// Surrogate pricer on the B200 tensor cores (include/fpe_surrogate.h).
+//
+// Every dense product of the MLP -- forward, input gradient and weight
+// gradient -- is one shape of kernel: C[M x N] = A[M x K] B[N x K]^T with both
+// operands BF16 and K-contiguous ("K-major"), FP32 accumulation in tensor
+// memory.  The backward pass keeps feature-major (transposed) copies of the
+// activations and gradients, written by the producing epilogues, so that the
+// weight gradients are K-major products over the batch as well.
+//
+// One CTA of 128 threads computes a 128 x N tile (N <= 256): K is staged in
+// 64-wide chunks into two shared-memory buffers in the canonical no-swizzle
+// K-major layout (8-row x 16-byte core matrices), one thread issues
+// tcgen05.mma (M = 128, N, K = 16) into a TMEM accumulator and commits to an
+// mbarrier, the next chunk loads while the MMAs run, and the epilogue reads
+// the accumulator back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31,
+// i.e. tile rows) and applies bias / SiLU / SiLU' before storing.
+//
+// Adam follows the reference update rule (src/nn/adam.mojo:31-64).
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/fpe_surrogate.h"
+#include "bulk_pipe.cuh"
+
+namespace fpe {
+namespace mlp {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kTileM = 128;
+constexpr int kTileN = 256;
+constexpr int kChunkK = 64;
+constexpr int kThreads = 128;
+constexpr int kBufBytes = (kTileM + kTileN) * kChunkK * 2;  // one A + B chunk
+constexpr int kSmemBytes = 2 * kBufBytes;                    // double buffered (96 KB: <= 2 CTAs per SM)
+
+// ---- tcgen05 helpers ---------------------------------------------------------
+// Shared-memory matrix descriptor: start address, leading-dimension byte
+// offset (between the two 8-element K halves of an MMA step) and stride byte
+// offset (between 8-row groups), all >> 4; descriptor version 1; no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= uint64_t((saddr >> 4) & 0x3FFFu);
+  d |= uint64_t((lbo >> 4) & 0x3FFFu) << 16;
+  d |= uint64_t((sbo >> 4) & 0x3FFFu) << 32;
+  d |= uint64_t(1) << 46;
+  return d;
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Warp-wide: allocate ncols TMEM columns, address written to *slot (shared).
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t"
+      ".reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+      "}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(unsigned long long* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+// 16 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + __expf(-z)); }
+
+// ---- the product kernel --------------------------------------------------------
+enum Epi : int {
+  EPI_F32 = 0,        // Cf = A B^T (+ bias) (optionally SiLU)
+  EPI_BIAS_SILU = 1,  // z = A B^T + bias: Cf = z (optional), Cb / CbT = bf16(silu(z))
+  EPI_DSILU = 2,      // g = (A B^T) .* silu'(zin): Cf = g (optional), Cb / CbT = bf16(g)
+};
+
+struct GemmParams {
+  const bf16* A;
+  int lda;
+  const bf16* B;
+  int ldb;
+  int M, N, K;
+  int epi;
+  int act;           // EPI_F32: 1 applies SiLU
+  const float* bias;  // N, or null
+  const float* zin;   // EPI_DSILU: M x N pre-activations (ldz)
+  int ldz;
+  float* Cf;
+  int ldcf;
+  bf16* Cb;
+  int ldcb;
+  bf16* CbT;  // transposed (N x M)
+  int ldcbt;
+  int* err;
+};
+
+// Stage rows [row0, row0 + rows) x K [k0, k0 + kc) of a K-contiguous BF16
+// matrix into the canonical layout: core matrix (row / 8, k / 8) at
+// ((row / 8) * (kc / 8) + k / 8) * 128 bytes, row % 8 at 16 bytes each.
+__device__ __forceinline__ void stage_kmajor(unsigned char* dst, const bf16* src, int ld, int row0, int rows,
+                                             int k0, int kc) {
+  const int k8n = kc >> 3;
+  for (int v = threadIdx.x; v < rows * k8n; v += blockDim.x) {
+    const int r = v / k8n, j = v - r * k8n;
+    const uint4 val = *reinterpret_cast<const uint4*>(src + size_t(row0 + r) * ld + k0 + 8 * j);
+    *reinterpret_cast<uint4*>(dst + ((r >> 3) * k8n + j) * 128 + (r & 7) * 16) = val;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ unsigned long long bar[2];
+  __shared__ uint32_t tmem_slot;
+  const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * kTileN;
+  const int Nt = min(kTileN, P.N - n0);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  uint32_t ncols = 32;
+  while (int(ncols) < Nt) ncols <<= 1;
+  unsigned char* bufA[2] = {smem, smem + kBufBytes};
+  unsigned char* bufB[2] = {smem + kTileM * kChunkK * 2, smem + kBufBytes + kTileM * kChunkK * 2};
+
+  if (warp == 0) tmem_alloc(&tmem_slot, ncols);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  const int nchunk = (P.K + kChunkK - 1) / kChunkK;
+  const uint32_t idesc = umma_idesc_bf16(kTileM, Nt);
+  uint32_t phase = 0;
+  bool ok = true;
+  auto load = [&](int c, int b) {
+    const int k0 = c * kChunkK, kc = min(kChunkK, P.K - k0);
+    stage_kmajor(bufA[b], P.A, P.lda, m0, kTileM, k0, kc);
+    stage_kmajor(bufB[b], P.B, P.ldb, n0, Nt, k0, kc);
+  };
+  load(0, 0);
+  fence_proxy_async_smem();
+  __syncthreads();
+  for (int c = 0; c < nchunk; ++c) {
+    const int b = c & 1;
+    if (c >= 1) {  // the MMAs of chunk c - 1 are done: buffer b ^ 1 is free
+      const int bp = b ^ 1;
+      if (mbar_wait_bounded(&bar[bp], (phase >> bp) & 1u, kBulkWaitLimit)) {
+        phase ^= 1u << bp;
+      } else {
+        ok = false;
+      }
+      tc_fence_after();
+    }
+    if (tid == 0 && ok) {
+      tc_fence_after();
+      const int k0 = c * kChunkK, kc = min(kChunkK, P.K - k0), k8n = kc >> 3;
+      const uint32_t sa = smem_u32(bufA[b]), sb = smem_u32(bufB[b]);
+      for (int s = 0; s < (kc >> 4); ++s) {
+        const uint64_t ad = umma_desc(sa + 256u * s, 128u, uint32_t(k8n) * 128u);
+        const uint64_t bd = umma_desc(sb + 256u * s, 128u, uint32_t(k8n) * 128u);
+        umma_bf16(tmem, ad, bd, idesc, (c > 0 || s > 0) ? 1u : 0u);
+      }
+      umma_commit(&bar[b]);
+    }
+    if (c + 1 < nchunk) load(c + 1, b ^ 1);
+    fence_proxy_async_smem();
+    __syncthreads();
+  }
+  {
+    const int bl = (nchunk - 1) & 1;
+    if (mbar_wait_bounded(&bar[bl], (phase >> bl) & 1u, kBulkWaitLimit)) {
+      phase ^= 1u << bl;
+    } else {
+      ok = false;
+    }
+    tc_fence_after();
+  }
+  ok = __syncthreads_and(ok ? 1 : 0) != 0;
+  if (ok) {
+    const int r = 32 * warp + lane;
+    const int gm = m0 + r;
+    const uint32_t trow = tmem + (uint32_t(32 * warp) << 16);
+    for (int c = 0; c < Nt; c += 16) {
+      float v[16];
+      tmem_ld16(trow + uint32_t(c), v);
+      const int gn = n0 + c;
+      if (P.epi == EPI_F32) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          float z = v[j] + (P.bias ? P.bias[gn + j] : 0.0f);
+          if (P.act) z = z * sigmoidf_(z);
+          v[j] = z;
+        }
+      } else if (P.epi == EPI_BIAS_SILU) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] += P.bias ? P.bias[gn + j] : 0.0f;
+      } else {
+        const float* zr = P.zin + size_t(gm) * P.ldz + gn;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const float z = zr[j], s = sigmoidf_(z);
+          v[j] *= s * (1.0f + z * (1.0f - s));
+        }
+      }
+      if (P.Cf) {
+        float4* d = reinterpret_cast<float4*>(P.Cf + size_t(gm) * P.ldcf + gn);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      }
+      if (P.Cb || P.CbT) {
+        bf16 h[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const float x = P.epi == EPI_BIAS_SILU ? v[j] * sigmoidf_(v[j]) : v[j];
+          h[j] = __float2bfloat16_rn(x);
+        }
+        if (P.Cb) {
+          uint4* d = reinterpret_cast<uint4*>(P.Cb + size_t(gm) * P.ldcb + gn);
+          d[0] = *reinterpret_cast<const uint4*>(&h[0]);
+          d[1] = *reinterpret_cast<const uint4*>(&h[8]);
+        }
+        if (P.CbT) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) P.CbT[size_t(gn + j) * P.ldcbt + gm] = h[j];
+        }
+      }
+    }
+  } else if (tid == 0 && P.err) {
+    atomicExch(P.err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, ncols);
+  }
+}
+
+// ---- small kernels of the MLP -----------------------------------------------------
+// X fp32 (n x n_in) -> BF16 (rows x in_pad) and its transpose; rows >= n and
+// columns >= n_in are zero.
+__global__ void k_pack_input(const float* __restrict__ x, int n, int n_in, int in_pad, int rows,
+                             bf16* __restrict__ X, bf16* __restrict__ XT) {
+  const int total = rows * in_pad;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int r = e / in_pad, c = e - r * in_pad;
+    const float v = (r < n && c < n_in) ? x[size_t(r) * n_in + c] : 0.0f;
+    const bf16 b = __float2bfloat16_rn(v);
+    X[e] = b;
+    if (XT) XT[size_t(c) * rows + r] = b;
+  }
+}
+
+// y_hat[r] = sum_j H[r][j] w[j] + b, one warp per row.
+__global__ void k_out_forward(const bf16* __restrict__ H, int hidden, int rows, const float* __restrict__ w,
+                              const float* __restrict__ b, float* __restrict__ y) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= rows) return;
+  const bf16* h = H + size_t(warp) * hidden;
+  float acc = 0.0f;
+  for (int j = lane; j < hidden; j += 32) acc = fmaf(__bfloat162float(h[j]), w[j], acc);
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) y[warp] = acc + b[0];
+}
+
+// dy[r] = 2 w_r (y_hat - y) / n (zero for padded rows); loss += w_r (y_hat - y)^2 / n.
+__global__ void k_loss_grad(const float* __restrict__ yhat, const float* __restrict__ y,
+                            const float* __restrict__ wt, int n, int rows, float* __restrict__ dy,
+                            float* __restrict__ loss) {
+  float part = 0.0f;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    float g = 0.0f;
+    if (r < n) {
+      const float e = yhat[r] - y[r], w = wt ? wt[r] : 1.0f;
+      g = 2.0f * w * e / float(n);
+      part += w * e * e / float(n);
+    }
+    dy[r] = g;
+  }
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+  if ((threadIdx.x & 31) == 0 && loss) atomicAdd(loss, part);
+}
+
+// Output layer backward: dZ[r][j] = dy[r] w[j] silu'(Z[r][j]) (fp32, bf16, bf16^T).
+__global__ void k_out_backward(const float* __restrict__ dy, const float* __restrict__ w,
+                               const float* __restrict__ Z, int rows, int hidden, float* __restrict__ dZ,
+                               bf16* __restrict__ dZb, bf16* __restrict__ dZbT) {
+  const int total = rows * hidden;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int r = e / hidden, j = e - r * hidden;
+    const float z = Z[e], s = sigmoidf_(z);
+    const float g = dy[r] * w[j] * s * (1.0f + z * (1.0f - s));
+    dZ[e] = g;
+    const bf16 b = __float2bfloat16_rn(g);
+    dZb[e] = b;
+    dZbT[size_t(j) * rows + r] = b;
+  }
+}
+
+// out[j] = sum_r X[r][j] (* s[r]) over rows, one block of 256 threads per 32
+// columns: 8 row-slices x 32 columns, then a shared-memory reduction.
+template <typename T>
+__global__ void k_colsum(const T* __restrict__ X, int ld, int rows, int cols, const float* __restrict__ s,
+                         float* __restrict__ out) {
+  __shared__ float red[8][33];
+  const int c = blockIdx.x * 32 + (threadIdx.x & 31), slice = threadIdx.x >> 5;
+  float acc = 0.0f;
+  if (c < cols) {
+    for (int r = slice; r < rows; r += 8) {
+      float x;
+      if constexpr (sizeof(T) == 2) {
+        x = __bfloat162float(X[size_t(r) * ld + c]);
+      } else {
+        x = X[size_t(r) * ld + c];
+      }
+      acc = fmaf(x, s ? s[r] : 1.0f, acc);
+    }
+  }
+  red[slice][threadIdx.x & 31] = acc;
+  __syncthreads();
+  if (slice == 0 && c < cols) {
+    float t = 0.0f;
+    for (int k = 0; k < 8; ++k) t += red[k][threadIdx.x & 31];
+    out[c] = t;
+  }
+}
+
+__global__ void k_sum(const float* __restrict__ x, int n, float* __restrict__ out) {
+  __shared__ float red[32];
+  float acc = 0.0f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += x[i];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int k = 0; k < int(blockDim.x >> 5); ++k) t += red[k];
+    out[0] = t;
+  }
+}
+
+// Adam (reference src/nn/adam.mojo:31-64): m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2,
+// theta -= lr * (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps).
+__global__ void k_adam(float* __restrict__ theta, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps, float c1,
+                       float c2) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    theta[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+// BF16 copies of a weight matrix W (out x in, row-major) and of its transpose.
+__global__ void k_cast_weights(const float* __restrict__ W, int out, int in, bf16* __restrict__ Wb,
+                               bf16* __restrict__ WbT) {
+  const int total = out * in;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int o = e / in, i = e - o * in;
+    const bf16 b = __float2bfloat16_rn(W[e]);
+    Wb[e] = b;
+    WbT[size_t(i) * out + o] = b;
+  }
+}
+
+}  // namespace mlp
+}  // namespace fpe
+
+// =====================================================================================
+// Host side
+// =====================================================================================
+namespace {
+
+using fpe::mlp::bf16;
+
+#define MK(x)                                                                       \
+  do {                                                                              \
+    cudaError_t e_ = (x);                                                           \
+    if (e_ != cudaSuccess) {                                                        \
+      if (std::getenv("FPE_DEBUG"))                                                 \
+        std::fprintf(stderr, "fpe_mlp: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(e_), \
+                     __FILE__, __LINE__);                                           \
+      return -1;                                                                    \
+    }                                                                               \
+  } while (0)
+
+struct MlpCtx {
+  bool ok = false;
+  cudaStream_t stream = nullptr;
+};
+
+MlpCtx& mctx() {
+  static MlpCtx c;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return;
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return;
+    if (cudaFuncSetAttribute(fpe::mlp::k_gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             fpe::mlp::kSmemBytes) != cudaSuccess)
+      return;
+    c.ok = true;
+  });
+  return c;
+}
+
+int launch_gemm(const fpe::mlp::GemmParams& P, cudaStream_t s) {
+  using namespace fpe::mlp;
+  if (P.M <= 0 || P.N <= 0 || P.K <= 0 || P.M % kTileM || P.N % 16 || P.K % 16 || P.lda % 8 || P.ldb % 8)
+    return -1;
+  if ((reinterpret_cast<uintptr_t>(P.A) | reinterpret_cast<uintptr_t>(P.B)) & 15) return -1;
+  if (P.Cf && (P.ldcf % 4 || (reinterpret_cast<uintptr_t>(P.Cf) & 15))) return -1;
+  if (P.Cb && (P.ldcb % 8 || (reinterpret_cast<uintptr_t>(P.Cb) & 15))) return -1;
+  const dim3 grid(P.M / kTileM, (P.N + kTileN - 1) / kTileN);
+  k_gemm_bf16_tc<<<grid, kThreads, kSmemBytes, s>>>(P);
+  MK(cudaGetLastError());
+  return 0;
+}
+
+fpe::mlp::GemmParams gp(const bf16* A, int lda, const bf16* B, int ldb, int M, int N, int K, int epi, int* err) {
+  fpe::mlp::GemmParams P{};
+  P.A = A;
+  P.lda = lda;
+  P.B = B;
+  P.ldb = ldb;
+  P.M = M;
+  P.N = N;
+  P.K = K;
+  P.epi = epi;
+  P.err = err;
+  return P;
+}
+
+inline int grid_for(int64_t n, int block = 256) {
+  const int64_t g = (n + block - 1) / block;
+  return int(g < 1 ? 1 : (g > 148 * 32 ? 148 * 32 : g));
+}
+
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+}  // namespace
+
+struct FpeMlp {
+  int n_in = 0, in_pad = 0, hidden = 0, layers = 0, rows = 0;  // rows: max rows per call (multiple of 128)
+  int64_t n_params = 0;
+  std::vector<int64_t> off_w, off_b;  // per hidden layer
+  int64_t off_wo = 0, off_bo = 0;
+  float *theta = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
+  std::vector<bf16*> Wb, WbT;
+  bf16 *X = nullptr, *XT = nullptr;
+  std::vector<float*> Z;
+  std::vector<bf16*> H, HT;
+  float *dZ[2] = {nullptr, nullptr};
+  bf16 *dZb[2] = {nullptr, nullptr}, *dZbT[2] = {nullptr, nullptr};
+  float *yhat = nullptr, *dy = nullptr, *loss = nullptr;
+  int* err = nullptr;
+  int64_t step = 0;
+  std::vector<void*> allocs;
+
+  int in_of(int l) const { return l == 0 ? in_pad : hidden; }
+  template <typename T>
+  int alloc(T** p, size_t count) {
+    void* q = nullptr;
+    MK(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)));
+    MK(cudaMemset(q, 0, std::max<size_t>(count, 1) * sizeof(T)));
+    allocs.push_back(q);
+    *p = static_cast<T*>(q);
+    return 0;
+  }
+  ~FpeMlp() {
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+namespace {
+
+int mlp_cast_all(FpeMlp* M, cudaStream_t s) {
+  for (int l = 0; l < M->layers; ++l) {
+    const int in = M->in_of(l);
+    fpe::mlp::k_cast_weights<<<grid_for(int64_t(M->hidden) * in), 256, 0, s>>>(
+        M->theta + M->off_w[l], M->hidden, in, M->Wb[l], M->WbT[l]);
+  }
+  MK(cudaGetLastError());
+  return 0;
+}
+
+// Forward over rows [0, rows) of the packed input; keep = 1 stores Z and H^T
+// (training), otherwise only H (inference).
+int mlp_forward_packed(FpeMlp* M, int rows, bool keep, cudaStream_t s) {
+  using namespace fpe::mlp;
+  const bf16* in = M->X;
+  int ld_in = M->in_pad;
+  for (int l = 0; l < M->layers; ++l) {
+    GemmParams P = gp(in, ld_in, M->Wb[l], M->in_of(l), rows, M->hidden, M->in_of(l), EPI_BIAS_SILU, M->err);
+    P.bias = M->theta + M->off_b[l];
+    P.Cb = keep ? M->H[l] : M->H[l & 1];
+    P.ldcb = M->hidden;
+    if (keep) {
+      P.Cf = M->Z[l];
+      P.ldcf = M->hidden;
+      P.CbT = M->HT[l];
+      P.ldcbt = M->rows;
+    }
+    if (launch_gemm(P, s)) return -1;
+    in = P.Cb;
+    ld_in = M->hidden;
+  }
+  const bf16* last = keep ? M->H[M->layers - 1] : M->H[(M->layers - 1) & 1];
+  k_out_forward<<<(rows * 32 + 255) / 256, 256, 0, s>>>(last, M->hidden, rows, M->theta + M->off_wo,
+                                                         M->theta + M->off_bo, M->yhat);
+  MK(cudaGetLastError());
+  return 0;
+}
+
+// Forward + backward: gradient of sum_i w_i (y_hat_i - y_i)^2 / n into M->grad,
+// loss into M->loss.
+int mlp_backward(FpeMlp* M, const float* x, const float* y, const float* w, int n, cudaStream_t s) {
+  using namespace fpe::mlp;
+  const int R = M->rows, Hd = M->hidden;
+  k_pack_input<<<grid_for(int64_t(R) * M->in_pad), 256, 0, s>>>(x, n, M->n_in, M->in_pad, R, M->X, M->XT);
+  MK(cudaGetLastError());
+  if (mlp_forward_packed(M, R, true, s)) return -1;
+  MK(cudaMemsetAsync(M->loss, 0, sizeof(float), s));
+  k_loss_grad<<<grid_for(R), 256, 0, s>>>(M->yhat, y, w, n, R, M->dy, M->loss);
+  const int L = M->layers;
+  // output layer
+  k_colsum<bf16><<<(Hd + 31) / 32, 256, 0, s>>>(M->H[L - 1], Hd, R, Hd, M->dy, M->grad + M->off_wo);
+  k_sum<<<1, 256, 0, s>>>(M->dy, R, M->grad + M->off_bo);
+  int cur = 0;
+  k_out_backward<<<grid_for(int64_t(R) * Hd), 256, 0, s>>>(M->dy, M->theta + M->off_wo, M->Z[L - 1], R, Hd,
+                                                             M->dZ[cur], M->dZb[cur], M->dZbT[cur]);
+  MK(cudaGetLastError());
+  for (int l = L - 1; l >= 0; --l) {
+    const int in = M->in_of(l);
+    // dW_l = dZ_l^T H_{l-1}: A = dZ_l^T (hidden x R), B = H_{l-1}^T (in x R)
+    const bf16* Bt = l == 0 ? M->XT : M->HT[l - 1];
+    GemmParams P = gp(M->dZbT[cur], R, Bt, R, Hd, in, R, EPI_F32, M->err);
+    P.Cf = M->grad + M->off_w[l];
+    P.ldcf = in;
+    if (launch_gemm(P, s)) return -1;
+    k_colsum<float><<<(Hd + 31) / 32, 256, 0, s>>>(M->dZ[cur], Hd, R, Hd, nullptr, M->grad + M->off_b[l]);
+    if (l > 0) {
+      // dZ_{l-1} = (dZ_l W_l) .* silu'(Z_{l-1}): A = dZ_l (R x hidden), B = W_l^T (hidden x hidden)
+      GemmParams Q = gp(M->dZb[cur], Hd, M->WbT[l], Hd, R, Hd, Hd, EPI_DSILU, M->err);
+      Q.zin = M->Z[l - 1];
+      Q.ldz = Hd;
+      Q.Cf = M->dZ[cur ^ 1];
+      Q.ldcf = Hd;
+      Q.Cb = M->dZb[cur ^ 1];
+      Q.ldcb = Hd;
+      Q.CbT = M->dZbT[cur ^ 1];
+      Q.ldcbt = R;
+      if (launch_gemm(Q, s)) return -1;
+      cur ^= 1;
+    }
+  }
+  MK(cudaGetLastError());
+  return 0;
+}
+
+int check_err(FpeMlp* M, cudaStream_t s) {
+  int h = 0;
+  MK(cudaMemcpyAsync(&h, M->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MK(cudaStreamSynchronize(s));
+  return h ? -2 : 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+FpeMlp* fpe_mlp_create(int32_t n_in, int32_t hidden, int32_t layers, int32_t max_rows, uint64_t seed) {
+  if (n_in <= 0 || n_in > 256 || (hidden != 128 && hidden != 256) || layers < 1 || layers > 16 ||
+      max_rows <= 0)
+    return nullptr;
+  if (!mctx().ok) return nullptr;
+  auto* M = new FpeMlp();
+  M->n_in = n_in;
+  M->in_pad = (n_in + 15) & ~15;
+  M->hidden = hidden;
+  M->layers = layers;
+  M->rows = (max_rows + 127) & ~127;
+  int64_t o = 0;
+  for (int l = 0; l < layers; ++l) {
+    M->off_w.push_back(o);
+    o += int64_t(hidden) * M->in_of(l);
+    M->off_b.push_back(o);
+    o += hidden;
+  }
+  M->off_wo = o;
+  o += hidden;
+  M->off_bo = o;
+  o += 1;
+  M->n_params = o;
+  // host init: U(-1/sqrt(fan_in), 1/sqrt(fan_in)), padded input columns zero
+  std::vector<float> h(size_t(o), 0.0f);
+  uint64_t st = seed * 0x2545F4914F6CDD1Dull + 1;
+  auto uni = [&](float a) { return float((double(splitmix(st) >> 11) * 0x1.0p-53 * 2.0 - 1.0) * a); };
+  for (int l = 0; l < layers; ++l) {
+    const int fan = l == 0 ? n_in : hidden, in = M->in_of(l);
+    const float a = 1.0f / std::sqrt(float(fan));
+    for (int r = 0; r < hidden; ++r)
+      for (int c = 0; c < fan; ++c) h[size_t(M->off_w[l] + int64_t(r) * in + c)] = uni(a);
+    for (int r = 0; r < hidden; ++r) h[size_t(M->off_b[l] + r)] = uni(a);
+  }
+  {
+    const float a = 1.0f / std::sqrt(float(hidden));
+    for (int r = 0; r < hidden; ++r) h[size_t(M->off_wo + r)] = uni(a);
+    h[size_t(M->off_bo)] = uni(a);
+  }
+  bool bad = M->alloc(&M->theta, o) || M->alloc(&M->grad, o) || M->alloc(&M->m, o) || M->alloc(&M->v, o);
+  M->Wb.resize(layers);
+  M->WbT.resize(layers);
+  M->Z.resize(layers);
+  M->H.resize(layers);
+  M->HT.resize(layers);
+  const size_t R = size_t(M->rows);
+  for (int l = 0; l < layers && !bad; ++l) {
+    const size_t wsz = size_t(hidden) * M->in_of(l);
+    bad = M->alloc(&M->Wb[l], wsz) || M->alloc(&M->WbT[l], wsz) || M->alloc(&M->Z[l], R * hidden) ||
+          M->alloc(&M->H[l], R * hidden) || M->alloc(&M->HT[l], R * hidden);
+  }
+  for (int k = 0; k < 2 && !bad; ++k)
+    bad = M->alloc(&M->dZ[k], R * hidden) || M->alloc(&M->dZb[k], R * hidden) || M->alloc(&M->dZbT[k], R * hidden);
+  bad = bad || M->alloc(&M->X, R * M->in_pad) || M->alloc(&M->XT, R * M->in_pad) || M->alloc(&M->yhat, R) ||
+        M->alloc(&M->dy, R) || M->alloc(&M->loss, 1) || M->alloc(&M->err, 1);
+  if (bad || cudaMemcpy(M->theta, h.data(), size_t(o) * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+      mlp_cast_all(M, mctx().stream) || cudaStreamSynchronize(mctx().stream) != cudaSuccess) {
+    delete M;
+    return nullptr;
+  }
+  return M;
+}
+
+void fpe_mlp_destroy(FpeMlp* M) {
+  if (!M) return;
+  cudaDeviceSynchronize();
+  delete M;
+}
+
+int64_t fpe_mlp_layout(const FpeMlp* M, int32_t* layout) {
+  if (!M) return -1;
+  if (layout) {
+    layout[0] = M->n_in;
+    layout[1] = M->in_pad;
+    layout[2] = M->hidden;
+    layout[3] = M->layers;
+  }
+  return M->n_params;
+}
+
+int32_t fpe_mlp_get_params(FpeMlp* M, float* out, int64_t n) {
+  if (!M || !out || n != M->n_params) return -1;
+  MK(cudaStreamSynchronize(mctx().stream));
+  MK(cudaMemcpy(out, M->theta, size_t(n) * sizeof(float), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int32_t fpe_mlp_set_params(FpeMlp* M, const float* in, int64_t n) {
+  if (!M || !in || n != M->n_params) return -1;
+  cudaStream_t s = mctx().stream;
+  MK(cudaStreamSynchronize(s));
+  MK(cudaMemcpy(M->theta, in, size_t(n) * sizeof(float), cudaMemcpyHostToDevice));
+  MK(cudaMemset(M->m, 0, size_t(n) * sizeof(float)));
+  MK(cudaMemset(M->v, 0, size_t(n) * sizeof(float)));
+  M->step = 0;
+  if (mlp_cast_all(M, s)) return -1;
+  MK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int32_t fpe_mlp_forward(FpeMlp* M, const float* x, int32_t n, float* y, void* stream) {
+  if (!M || !x || !y || n < 0) return -1;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : mctx().stream;
+  for (int32_t r0 = 0; r0 < n; r0 += M->rows) {
+    const int cnt = std::min(M->rows, n - r0);
+    const int rows = (cnt + 127) & ~127;
+    fpe::mlp::k_pack_input<<<grid_for(int64_t(rows) * M->in_pad), 256, 0, s>>>(
+        x + size_t(r0) * M->n_in, cnt, M->n_in, M->in_pad, rows, M->X, nullptr);
+    if (mlp_forward_packed(M, rows, false, s)) return -1;
+    MK(cudaMemcpyAsync(y + r0, M->yhat, size_t(cnt) * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  }
+  MK(cudaGetLastError());
+  return 0;
+}
+
+int32_t fpe_mlp_train_step(FpeMlp* M, const float* x, const float* y, const float* w, int32_t n, float lr,
+                           float* loss_dev, void* stream) {
+  if (!M || !x || !y || n <= 0 || n > M->rows) return -1;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : mctx().stream;
+  if (mlp_backward(M, x, y, w, n, s)) return -1;
+  if (loss_dev) MK(cudaMemcpyAsync(loss_dev, M->loss, sizeof(float), cudaMemcpyDeviceToDevice, s));
+  M->step += 1;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - std::pow(b1, float(M->step)), c2 = 1.0f - std::pow(b2, float(M->step));
+  fpe::mlp::k_adam<<<grid_for(M->n_params), 256, 0, s>>>(M->theta, M->grad, M->m, M->v, M->n_params, lr, b1, b2,
+                                                          1e-8f, c1, c2);
+  MK(cudaGetLastError());
+  return mlp_cast_all(M, s);
+}
+
+int32_t fpe_mlp_gradient(FpeMlp* M, const float* x, const float* y, const float* w, int32_t n, float* grad_host,
+                         float* loss_host) {
+  if (!M || !x || !y || n <= 0 || n > M->rows || !grad_host) return -1;
+  cudaStream_t s = mctx().stream;
+  MK(cudaMemsetAsync(M->err, 0, sizeof(int), s));
+  if (mlp_backward(M, x, y, w, n, s)) return -1;
+  MK(cudaMemcpyAsync(grad_host, M->grad, size_t(M->n_params) * sizeof(float), cudaMemcpyDeviceToHost, s));
+  if (loss_host) MK(cudaMemcpyAsync(loss_host, M->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+  return check_err(M, s);
+}
+
+int32_t fpe_gemm_bf16(const void* a, int32_t lda, const void* b, int32_t ldb, int32_t M, int32_t N, int32_t K,
+                      const float* bias, int32_t act, float* c, int32_t ldc, void* stream) {
+  if (!a || !b || !c) return -1;
+  if (!mctx().ok) return -1;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : mctx().stream;
+  static int* d_err = nullptr;
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!d_err) MK(cudaMalloc(&d_err, sizeof(int)));
+  }
+  MK(cudaMemsetAsync(d_err, 0, sizeof(int), s));
+  fpe::mlp::GemmParams P = gp(static_cast<const bf16*>(a), lda, static_cast<const bf16*>(b), ldb, M, N, K,
+                              fpe::mlp::EPI_F32, d_err);
+  P.bias = bias;
+  P.act = act;
+  P.Cf = c;
+  P.ldcf = ldc;
+  if (launch_gemm(P, s)) return -1;
+  int h = 0;
+  MK(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MK(cudaStreamSynchronize(s));
+  return h ? -2 : 0;
+}
+
+}  // extern "C"

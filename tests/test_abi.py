@@ -1,5 +1,5 @@
 """C ABI and host-side logic, CPU only: the library builds, loads and exports
-every symbol include/fpe_engine.h declares, struct layouts match the
+every symbol include/*.h declares, struct layouts match the
 reference header, parameter validation mirrors the reference bindings, and
 nothing computes without a GPU (no CPU fallback)."""
 import ctypes as C
@@ -9,13 +9,16 @@ import re
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "fpe_engine.h")
+INCLUDE = os.path.join(ROOT, "include")
+HEADERS = sorted(os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h"))
 
 
 def _header_functions():
-    src = open(HEADER).read()
-    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(fpe_[a-z0-9_]+)\s*\(", src)))
+    names = set()
+    for h in HEADERS:
+        src = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        names.update(re.findall(r"\b(fpe_[a-z0-9_]+)\s*\(", src))
+    return sorted(names)
 
 
 @pytest.fixture(scope="module")
@@ -51,9 +54,10 @@ def test_reference_struct_layouts():
 def test_header_compiles_as_c_and_cpp(tmp_path):
     import subprocess
 
+    includes = "".join(f'#include "{os.path.basename(h)}"\n' for h in HEADERS)
     for comp, ext in (("gcc", "c"), ("g++", "cpp")):
         src = tmp_path / f"t.{ext}"
-        src.write_text('#include "fpe_engine.h"\nint main(void){return 0;}\n')
+        src.write_text(includes + "int main(void){return 0;}\n")
         subprocess.run([comp, "-I", os.path.join(ROOT, "include"), "-c", str(src), "-o",
                         str(tmp_path / f"t_{ext}.o")], check=True)
 
