@@ -1,0 +1,264 @@
+"""Heston calibration by Levenberg-Marquardt on the B200 pricers.
+
+``levenberg_marquardt`` restates the reference optimizer
+(src/numerics/optim/lm.mojo:29-121): damped normal equations
+(J^T J + lambda I) delta = -J^T r, lambda starting at 1e-3, x10 after a
+rejected step and x0.1 (floored at 1e-10) after an accepted one, stop when
+||J^T r||_inf < tol.  Parameters are (kappa, theta, sigma, rho, V0) with the
+reference's clamps (src/engines/calibrator/calibrator.mojo:15-29) and a central
+finite-difference Jacobian (:64-74).
+
+Two residual back-ends price the whole surface per call:
+
+* ``FpeSurface``: the batched FPE solver.  A Jacobian is one GPU batch of
+  11 x (number of quotes) contracts (the base point and ten perturbed
+  parameter sets).  Its difference step is 1e-3 (1 + |x|), not the
+  reference's 1e-6: an adaptive-step solver at rtol 1e-6 changes its step
+  sequence between neighbouring parameter sets, which makes 1e-6 differences
+  noise.
+* ``SurrogateSurface``: the tensor-core MLP ensemble; a Jacobian costs
+  microseconds.  Its step is 2 % of the parameter's training range, coarser
+  than the BF16 rounding of the network's inputs.  Quotes the ensemble does
+  not trust (outside its box, or members disagreeing by more than the
+  pricer's tolerance) are priced by the FPE solver inside the loop.
+
+``calibrate_with_surrogate`` runs LM on the surrogate, then verifies the fit
+with one batched FPE pricing of the surface and, if the FPE residual is worse
+than the surrogate's by more than ``polish_ratio``, continues LM on the FPE
+solver from there.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PARAM_NAMES = ("kappa", "theta", "sigma", "rho", "V0")
+
+
+def clamp(x: np.ndarray) -> np.ndarray:
+    """Reference clamps (calibrator.mojo:15-29)."""
+    x = np.array(x, dtype=np.float64)
+    x[0] = max(x[0], 1e-4)
+    x[1] = max(x[1], 1e-5)
+    x[2] = max(x[2], 1e-4)
+    x[3] = min(0.999, max(-0.999, x[3]))
+    x[4] = max(x[4], 1e-6)
+    return x
+
+
+@dataclass
+class LMResult:
+    x: np.ndarray
+    iterations: int
+    residual_evals: int
+    cost: float
+    history: list = field(default_factory=list)
+
+
+def levenberg_marquardt(residual, jacobian, x0, max_iter: int = 50, tol: float = 1e-10,
+                        lambda_init: float = 1e-3, lambda_up: float = 10.0,
+                        lambda_down: float = 0.1, xtol: float | None = None) -> LMResult:
+    """Reference LM (lm.mojo:29-121).  jacobian(x) returns (r(x), J(x)).
+
+    xtol (not in the reference, off by default) also stops after an accepted
+    step with |delta|_inf <= xtol (|x|_inf + xtol): the test that ends a fit
+    whose residual cannot reach the gradient tolerance (a solver's rounding
+    and step-control noise)."""
+    x = np.array(x0, dtype=np.float64)
+    lam = lambda_init
+    evals = 0
+    hist = []
+    it = 0
+    cost = np.inf
+    for it in range(1, max_iter + 1):
+        r, J = jacobian(x)
+        evals += 1
+        g = J.T @ r
+        cost = float(r @ r)
+        hist.append((cost, lam))
+        if np.max(np.abs(g)) < tol:
+            break
+        A = J.T @ J + lam * np.eye(len(x))
+        delta = np.linalg.solve(A, -g)
+        x_new = x + delta
+        r_new = residual(x_new)
+        evals += 1
+        if float(r_new @ r_new) < cost:
+            x = x_new
+            lam = max(lam * lambda_down, 1e-10)
+            if xtol is not None and np.max(np.abs(delta)) <= xtol * (np.max(np.abs(x)) + xtol):
+                break
+        else:
+            lam = lam * lambda_up
+    return LMResult(x=x, iterations=it, residual_evals=evals, cost=cost, history=hist)
+
+
+@dataclass
+class Surface:
+    """Quotes of one underlying: strikes and maturities (flattened), market prices."""
+    S0: float
+    r: float
+    strikes: np.ndarray
+    maturities: np.ndarray
+    prices: np.ndarray
+    option_type: int = 8
+
+    @staticmethod
+    def grid(S0, r, k_over_s, maturities, option_type=8):
+        K, T = np.meshgrid(np.asarray(k_over_s) * S0, np.asarray(maturities), indexing="xy")
+        return Surface(S0, r, K.ravel(), T.ravel(), np.zeros(K.size), option_type)
+
+
+def contract_tables(surface: Surface, xs: np.ndarray, grid=(48, 24)):
+    """Contract tables for every parameter vector in xs (rows) over the surface."""
+    xs = np.atleast_2d(xs)
+    m = len(surface.strikes)
+    n = len(xs) * m
+    P = np.zeros((n, 12))
+    I = np.zeros((n, 3), np.int32)
+    for k, x in enumerate(xs):
+        x = clamp(x)
+        sl = slice(k * m, (k + 1) * m)
+        P[sl, 0], P[sl, 1], P[sl, 2], P[sl, 3] = x[0], x[1], x[2], x[3]
+        P[sl, 4] = surface.r
+        P[sl, 5] = surface.maturities
+        P[sl, 6] = surface.S0
+        P[sl, 7] = x[4]
+        P[sl, 8] = surface.strikes
+        P[sl, 11] = 3.0 * surface.S0
+    I[:, 0], I[:, 1] = grid
+    I[:, 2] = surface.option_type
+    return P, I
+
+
+class _Backend:
+    """Residuals r(x) = model(x) - market over the surface, and batched central
+    finite-difference Jacobians."""
+
+    def __init__(self, surface: Surface):
+        self.surface = surface
+        self.contracts_priced = 0
+        self.seconds = 0.0
+
+    def price_sets(self, xs: np.ndarray) -> np.ndarray:  # (len(xs), m)
+        raise NotImplementedError
+
+    def steps(self, x: np.ndarray) -> np.ndarray:
+        raise NotImplementedError
+
+    def residual(self, x):
+        return self.price_sets(np.atleast_2d(x))[0] - self.surface.prices
+
+    def jacobian(self, x):
+        x = np.asarray(x, np.float64)
+        h = self.steps(x)
+        xs = [x]
+        for j in range(len(x)):
+            for s in (+1.0, -1.0):
+                y = x.copy()
+                y[j] += s * h[j]
+                xs.append(y)
+        p = self.price_sets(np.array(xs))
+        r = p[0] - self.surface.prices
+        J = np.empty((len(r), len(x)))
+        for j in range(len(x)):
+            J[:, j] = (p[1 + 2 * j] - p[2 + 2 * j]) / (2.0 * h[j])
+        return r, J
+
+
+class FpeSurface(_Backend):
+    """Residuals from the batched FPE solver."""
+
+    def __init__(self, surface: Surface, options=None, grid=(48, 24), rel_step: float = 1e-3):
+        from . import BatchOptions
+
+        super().__init__(surface)
+        self.options = options or BatchOptions(disc=1, precision=1, rtol=1e-6, atol=1e-8,
+                                               complex_solve=2, radau_constants=2)
+        self.grid = grid
+        self.rel_step = rel_step
+
+    def steps(self, x):
+        return self.rel_step * (1.0 + np.abs(x))
+
+    def price_sets(self, xs):
+        from . import price_batch
+
+        t = time.perf_counter()
+        P, I = contract_tables(self.surface, xs, self.grid)
+        p, st = price_batch(P, I, self.options)
+        if np.any(st != 0):
+            raise RuntimeError(f"FPE pricing failed (status {sorted(set(st[st != 0].tolist()))})")
+        self.contracts_priced += len(P)
+        self.seconds += time.perf_counter() - t
+        return p.reshape(len(xs), -1)
+
+
+class SurrogateSurface(_Backend):
+    """Residuals from a SurrogatePricer (FPE fall-back for untrusted quotes).
+    Parameter vectors are projected into the surrogate's training box before
+    pricing, so the search never leaves the region the network was fitted on."""
+
+    # training box of (kappa, theta, sigma, rho, V0)
+    LO = np.array([0.5, 0.02, 0.1, -0.9, 0.02])
+    HI = np.array([3.0, 0.15, 0.8, 0.0, 0.2])
+    _RANGE = HI - LO
+
+    @classmethod
+    def project(cls, x):
+        return np.clip(np.asarray(x, np.float64), cls.LO, cls.HI)
+
+    def __init__(self, surface: Surface, pricer, grid=(48, 24), frac_step: float = 0.02):
+        super().__init__(surface)
+        self.pricer = pricer
+        self.grid = grid
+        self.frac_step = frac_step
+        self.fallback_quotes = 0
+
+    def steps(self, x):
+        return self.frac_step * self._RANGE
+
+    def price_sets(self, xs):
+        t = time.perf_counter()
+        P, I = contract_tables(self.surface, np.array([self.project(x) for x in np.atleast_2d(xs)]), self.grid)
+        p, fb = self.pricer.price(P, I)
+        self.fallback_quotes += int(fb.sum())
+        self.contracts_priced += int(fb.sum())  # FPE solves spent inside the loop
+        self.seconds += time.perf_counter() - t
+        return p.reshape(len(xs), -1)
+
+
+def calibrate_fpe(surface: Surface, x0, max_iter=40, tol=1e-10, xtol=1e-6, **kw):
+    be = FpeSurface(surface, **kw)
+    t = time.perf_counter()
+    res = levenberg_marquardt(be.residual, be.jacobian, x0, max_iter=max_iter, tol=tol, xtol=xtol)
+    return clamp(res.x), {"seconds": time.perf_counter() - t, "fpe_contracts": be.contracts_priced,
+                          "iterations": res.iterations, "cost": res.cost}
+
+
+def calibrate_with_surrogate(surface: Surface, pricer, x0, max_iter=50, tol=1e-10,
+                             polish_ratio: float = 2.0, polish_iter: int = 10, xtol=1e-6, fpe_kw=None):
+    """Surrogate-in-loop LM, FPE verification, optional FPE polish."""
+    fpe_kw = fpe_kw or {}
+    t = time.perf_counter()
+    sb = SurrogateSurface(surface, pricer, grid=fpe_kw.get("grid", (48, 24)))
+    res = levenberg_marquardt(sb.residual, sb.jacobian, SurrogateSurface.project(x0), max_iter=max_iter,
+                              tol=tol, xtol=1e-4)
+    x = clamp(SurrogateSurface.project(res.x))
+    fb = FpeSurface(surface, **fpe_kw)
+    r_fpe = fb.residual(x)
+    r_sur = sb.residual(x)
+    polished = False
+    it_polish = 0
+    if float(r_fpe @ r_fpe) > polish_ratio * max(float(r_sur @ r_sur), 1e-30):
+        pol = levenberg_marquardt(fb.residual, fb.jacobian, x, max_iter=polish_iter, tol=tol, xtol=xtol)
+        x = clamp(pol.x)
+        polished = True
+        it_polish = pol.iterations
+    return x, {"seconds": time.perf_counter() - t,
+               "fpe_contracts": fb.contracts_priced + sb.contracts_priced,
+               "surrogate_iterations": res.iterations, "polished": polished,
+               "polish_iterations": it_polish, "fallback_quotes": sb.fallback_quotes,
+               "fpe_rms_at_surrogate_fit": float(np.sqrt(np.mean(r_fpe ** 2)))}

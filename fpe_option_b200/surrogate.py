@@ -54,17 +54,27 @@ class Mlp:
             raise RuntimeError("fpe_mlp_set_params failed")
 
     # -- device-tensor entry points --------------------------------------------
+    def _stream(self, stream):
+        """The CUDA stream for a call: the given one, else torch's current stream
+        (its legacy default stream passed as cudaStreamLegacy), so that the
+        library's kernels are ordered with the torch ops around them."""
+        if stream is not None:
+            return stream
+        h = self._torch.cuda.current_stream().cuda_stream
+        return h if h else 1  # cudaStreamLegacy
+
     def forward_dev(self, x, y, stream: int | None = None) -> None:
         """y[n] = net(x[n, n_in]) for float32 CUDA tensors."""
         n = int(x.shape[0])
-        if self._L.fpe_mlp_forward(self._h, x.data_ptr(), n, y.data_ptr(), stream):
+        if self._L.fpe_mlp_forward(self._h, x.data_ptr(), n, y.data_ptr(), self._stream(stream)):
             raise RuntimeError("fpe_mlp_forward failed")
 
     def train_step_dev(self, x, t, w, lr: float, loss=None, stream: int | None = None) -> None:
         n = int(x.shape[0])
         rc = self._L.fpe_mlp_train_step(self._h, x.data_ptr(), t.data_ptr(),
                                         w.data_ptr() if w is not None else None, n, float(lr),
-                                        loss.data_ptr() if loss is not None else None, stream)
+                                        loss.data_ptr() if loss is not None else None,
+                                        self._stream(stream))
         if rc:
             raise RuntimeError("fpe_mlp_train_step failed")
 
@@ -89,6 +99,7 @@ class Mlp:
         tw = None if w is None else self._dev(w)
         g = np.empty(self.n_params, np.float32)
         loss = C.c_float(0.0)
+        self._torch.cuda.synchronize()  # the gradient call runs on the library's own stream
         rc = self._L.fpe_mlp_gradient(self._h, tx.data_ptr(), tt.data_ptr(),
                                       tw.data_ptr() if tw is not None else None, int(tx.shape[0]),
                                       g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss))
@@ -127,7 +138,11 @@ BOX_HI = np.array([3.0, 0.15, 0.8, 0.0, 0.2, 0.05, 2.0, 1.3, 1.4])
 # option types the surrogate covers: European call/put, down-and-out/in calls,
 # up-and-out/in puts
 SURROGATE_TYPES = (8, 9, 2, 0, 7, 5)
-PRICE_FLOOR = 2e-3  # in units of S0: floor of the relative-error weight
+# The network predicts y = log(price / S0 + LOG_EPS): squared error in y is a
+# relative-price error floored at LOG_EPS S0, and the BF16 rounding of the
+# activations (about 2^-9 relative) becomes a uniform relative price error
+# instead of an absolute one that would swamp small prices.
+LOG_EPS = 1e-3
 
 
 def encode(params: np.ndarray, ints: np.ndarray):
@@ -196,7 +211,7 @@ class SurrogateConfig:
     hidden: int = 256
     layers: int = 4
     batch: int = 4096
-    lr: float = 1e-3
+    lr: float = 1e-3       # peak learning rate, cosine-decayed to zero over the run
     epochs: int = 200
     disagreement_tol: float = 1e-3  # relative spread of the members that sends a query to the FPE solver
     seed: int = 0
@@ -233,10 +248,14 @@ class SurrogatePricer:
 
     @staticmethod
     def targets(params, prices):
-        """Training targets price / S0 and their relative-error weights."""
+        """Training targets log(price / S0 + LOG_EPS) and unit weights."""
         y = np.asarray(prices, np.float64) / np.asarray(params, np.float64)[:, 6]
-        w = 1.0 / (np.abs(y) + PRICE_FLOOR) ** 2
-        return y, w / w.mean()
+        y = np.log(np.maximum(y, 0.0) + LOG_EPS)
+        return y, np.ones_like(y)
+
+    @staticmethod
+    def to_price(y, S0):
+        return np.asarray(S0) * (np.exp(np.asarray(y, np.float64)) - LOG_EPS)
 
     # -- training -------------------------------------------------------------------
     def fit(self, params, ints, prices, epochs: int | None = None, log=None) -> list[float]:
@@ -251,19 +270,23 @@ class SurrogatePricer:
         tw = torch.as_tensor(w.astype(np.float32), device="cuda")
         n = len(x)
         bs = min(c.batch, n)
+        steps = max(1, epochs * (n // bs))
         losses = []
         for k, net in enumerate(self.members):
             gen = torch.Generator(device="cuda")
             gen.manual_seed(c.seed * 7919 + k)
             loss = torch.zeros(1, device="cuda")
+            step = 0
             for ep in range(epochs):
                 perm = torch.randperm(n, device="cuda", generator=gen)
                 acc = torch.zeros(1, device="cuda")
                 nb = 0
                 for s in range(0, n - bs + 1, bs):
                     idx = perm[s:s + bs]
+                    lr = 0.5 * c.lr * (1.0 + np.cos(np.pi * step / steps))
+                    step += 1
                     net.train_step_dev(tx[idx].contiguous(), ty[idx].contiguous(), tw[idx].contiguous(),
-                                       c.lr, loss)
+                                       lr, loss)
                     acc += loss
                     nb += 1
                 if log is not None and (ep + 1) % max(1, epochs // 5) == 0:
@@ -274,14 +297,16 @@ class SurrogatePricer:
 
     # -- inference --------------------------------------------------------------------
     def predict_features(self, x_dev):
-        """(mean, relative spread) of the members for a float32 CUDA feature tensor."""
+        """(mean log-price target, spread) of the members for a float32 CUDA
+        feature tensor; the spread max - min of the log targets is the members'
+        relative price disagreement."""
         torch = self._torch
         n = int(x_dev.shape[0])
         outs = torch.empty((len(self.members), n), device="cuda")
         for k, net in enumerate(self.members):
             net.forward_dev(x_dev, outs[k])
         mean = outs.mean(0)
-        spread = (outs.max(0).values - outs.min(0).values) / (mean.abs() + PRICE_FLOOR)
+        spread = outs.max(0).values - outs.min(0).values
         return mean, spread
 
     def price(self, params, ints):
@@ -292,7 +317,7 @@ class SurrogatePricer:
         mean, spread = self.predict_features(torch.as_tensor(x, device="cuda"))
         y = mean.cpu().numpy().astype(np.float64)
         ok = in_box & (spread.cpu().numpy() <= self.config.disagreement_tol)
-        prices = y * P[:, 6]
+        prices = self.to_price(y, P[:, 6])
         fb = ~ok
         if np.any(fb):
             prices[fb] = self.fpe_prices(P[fb], np.asarray(ints)[fb])
