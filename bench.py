@@ -181,9 +181,24 @@ def main():
     ap.add_argument("--precision", type=int, default=1)
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-sample", type=int, default=8,
+                    help="contracts timed on the plain one-solve-per-launch FP64 path")
+    ap.add_argument("--workload", default="batch", choices=["batch", "surrogate", "calibration"],
+                    help="batch: the batched FPE pricing line (default); surrogate / calibration: "
+                         "the learned part's measurements")
+    ap.add_argument("--train", type=int, default=65536, help="surrogate training prices")
+    ap.add_argument("--surrogate-file", default=None,
+                    help="calibration: load a trained European ensemble (npz) instead of training; "
+                         "if the file does not exist, train and save it there")
+    ap.add_argument("--epochs", type=int, default=None,
+                    help="surrogate epochs (default 200 for --workload surrogate, 2000 for calibration)")
+    ap.add_argument("--batch", type=int, default=None,
+                    help="surrogate batch (default 4096 for --workload surrogate, 1024 for calibration)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload != "batch":
+        return run_learned_workload(args)
 
     import torch
     import torch.distributed as dist
@@ -288,6 +303,24 @@ def main():
         cpu = {"value": rate, "unit": "prices/s", "cores": cores, "kind": "port",
                "sample": f"first {sample} contracts of the same batch, oracle C++ FP64 "
                          f"restatement on {cores} host threads, {dt:.1f} s"}
+    # ---- plain path: one contract per launch sequence, FP64 factors ---------------
+    plain = None
+    if rank == 0 and world == 1 and args.plain_sample > 0:
+        popts = fpe.BatchOptions(disc=1, precision=0, rtol=args.rtol, atol=args.rtol * 1e-2,
+                                 complex_solve=2, radau_constants=2)
+        m = min(args.plain_sample, nc)
+        one = [fpe.contracts_from_arrays(P[j:j + 1], I[j:j + 1]) for j in range(m)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for a1, k1 in one:
+            pl = fpe.Plan(a1, popts, _keep=k1)
+            pl.run(sptr)
+            pl.results()
+            pl.close()
+        dt = time.perf_counter() - t0
+        plain = {"value": m / dt, "unit": "prices/s", "sample": f"first {m} contracts of the batch, "
+                 "each its own plan and launch sequence, FP64 factors, same rtol",
+                 "batched_over_plain": value / (m / dt)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "prices/s", "n_gpus": world,
@@ -315,6 +348,7 @@ def main():
                          "traffic": traffic.get("bytes_per_launch") if traffic else None,
                          "algorithmic_bytes": int(stats["factor_bytes"])},
             "cpu_baseline": cpu,
+            "plain_fp64_one_per_launch": plain,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -324,6 +358,135 @@ def main():
         dist.destroy_process_group()
     return 0
 
+
+
+# ---------------------------------------------------------------------------------
+# The learned part: surrogate training / inference and calibration (1 GPU)
+# ---------------------------------------------------------------------------------
+SUR_GRID = (48, 24)
+
+
+def _fpe_options(fpe):
+    return fpe.BatchOptions(disc=1, precision=1, rtol=1e-6, atol=1e-8, complex_solve=2,
+                            radau_constants=2)
+
+
+def _train_surrogate(args, kind, n_train, log, epochs, batch):
+    """FPE training prices (timed), 90/10 split, ensemble training (timed)."""
+    import torch
+
+    import fpe_option_b200 as fpe
+    from fpe_option_b200.surrogate import SurrogateConfig, SurrogatePricer, draw_contracts, encode
+
+    pr = SurrogatePricer(SurrogateConfig(members=3, batch=batch, epochs=epochs, seed=args.seed),
+                         fpe_options=_fpe_options(fpe))
+    P, I = draw_contracts(n_train, seed=1000 + args.seed, kind=kind, grid=SUR_GRID)
+    t0 = time.perf_counter()
+    y = pr.fpe_prices(P, I)
+    t_gen = time.perf_counter() - t0
+    n_hold = n_train // 10
+    tr, ho = slice(n_hold, None), slice(0, n_hold)
+    t0 = time.perf_counter()
+    losses = pr.fit(P[tr], I[tr], y[tr], log=log)
+    t_fit = time.perf_counter() - t0
+    x = torch.as_tensor(encode(P[ho], I[ho])[0], device="cuda")
+    mean, spread = pr.predict_features(x)
+    got = pr.to_price(mean.cpu().numpy(), P[ho], I[ho])
+    ref = y[ho]
+    floor = 0.2  # 2e-3 S0
+    rel = np.abs(got - ref) / (np.abs(ref) + floor)
+    held = {"n": int(n_hold), "median_rel_err": float(np.median(rel)),
+            "p90_rel_err": float(np.quantile(rel, 0.9)), "max_rel_err": float(rel.max()),
+            "err_floor": floor, "trusted_frac": float(np.mean(spread.cpu().numpy() <= pr.config.disagreement_tol))}
+    return pr, {"train_prices": int(n_train - n_hold), "fpe_generation_s": t_gen,
+                "fpe_generation_prices_per_s": n_train / t_gen, "training_s": t_fit,
+                "final_losses": losses, "held_out": held}
+
+
+def run_learned_workload(args):
+    import torch
+
+    import fpe_option_b200 as fpe
+    from fpe_option_b200 import build
+
+    build.build_library()
+    if not fpe.is_available():
+        raise RuntimeError("CUDA engine unavailable")
+    log = (lambda m: print(m, file=sys.stderr, flush=True))
+    if args.workload == "surrogate":
+        from fpe_option_b200.surrogate import draw_contracts, encode
+
+        ep, bs = args.epochs or 200, args.batch or 4096
+        pr, info = _train_surrogate(args, "mixed", args.train, log, ep, bs)
+        nq = 1 << 20
+        Q, J = draw_contracts(nq, seed=7 + args.seed, kind="mixed", grid=SUR_GRID)
+        x = torch.as_tensor(encode(Q, J)[0], device="cuda")
+        for _ in range(max(args.warmup, 3)):
+            pr.predict_features(x)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            pr.predict_features(x)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        line = {"metric": "surrogate prices/s (3-member BF16 tensor-core ensemble) and held-out error vs FPE",
+                "value": nq / (ms / 1000.0), "unit": "prices/s", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": "bf16/f32",
+                "data": "synthetic", "workload": "surrogate",
+                "config": {"workload": f"{args.train} FPE prices ({SUR_GRID[0]}x{SUR_GRID[1]} grids, European "
+                                       "and barrier, 90/10 split), MLP 12-256x4-1 SiLU, Adam lr 1e-3 cosine, "
+                                       f"batch {bs}, {ep} epochs; inference on 1048576 random queries"},
+                **info}
+        print(json.dumps(line), flush=True)
+        pr.close()
+        return 0
+    # ---- calibration: 15 strikes x 8 maturities, FPE-only vs surrogate in the loop ----
+    from fpe_option_b200.calibration import Surface, calibrate_fpe, calibrate_with_surrogate, contract_tables
+
+    ep, bs = args.epochs or 2000, args.batch or 1024
+    if args.surrogate_file and os.path.exists(args.surrogate_file):
+        from fpe_option_b200.surrogate import SurrogateConfig, SurrogatePricer
+
+        pr = SurrogatePricer(SurrogateConfig(members=3, batch=bs, epochs=ep, seed=args.seed),
+                             fpe_options=_fpe_options(fpe))
+        pr.load(args.surrogate_file)
+        info = {"loaded": args.surrogate_file}
+    else:
+        pr, info = _train_surrogate(args, "european", args.train, log, ep, bs)
+        info["epochs"], info["batch"] = ep, bs
+        if args.surrogate_file:
+            pr.save(args.surrogate_file)
+    rng = np.random.default_rng(4242 + args.seed)
+    truth = np.array([rng.uniform(0.8, 2.5), rng.uniform(0.03, 0.12), rng.uniform(0.2, 0.7),
+                      rng.uniform(-0.8, -0.2), rng.uniform(0.03, 0.15)])
+    surf = Surface.grid(100.0, 0.02, np.linspace(0.7, 1.3, 15), np.linspace(0.1, 2.0, 8))
+    P, I = contract_tables(surf, truth, SUR_GRID)
+    p, st = fpe.price_batch(P, I, fpe.BatchOptions(disc=1, precision=0, rtol=1e-9, atol=1e-11,
+                                                   complex_solve=2, radau_constants=2))
+    assert (st == 0).all()
+    surf.prices = p + rng.normal(0.0, 1e-4 * 100.0, p.shape)
+    x0 = np.array([1.5, 0.08, 0.45, -0.45, 0.08])
+    kw = {"grid": SUR_GRID}
+    x_f, info_f = calibrate_fpe(surf, x0, **kw)
+    x_s, info_s = calibrate_with_surrogate(surf, pr, x0, max_iter=50, polish_iter=30, fpe_kw=kw,
+                                           quote_noise=1e-4 * 100.0)
+    err_f = np.abs(x_f - truth) / np.abs(truth)
+    err_s = np.abs(x_s - truth) / np.abs(truth)
+    line = {"metric": "Heston calibration wall time: surrogate-in-loop vs FPE-only (same GPU)",
+            "value": info_f["seconds"] / info_s["seconds"], "unit": "x speed-up", "n_gpus": 1,
+            "higher_is_better": True, "data": "synthetic", "workload": "calibration",
+            "config": {"workload": "15 strikes (K/S0 0.7-1.3) x 8 maturities (0.1-2.0), European calls, "
+                                   "FP64 FPE surface of a seeded parameter set + N(0, 1e-4 S0) noise, "
+                                   f"{SUR_GRID[0]}x{SUR_GRID[1]} grids"},
+            "truth": truth.tolist(),
+            "fpe_only": {**info_f, "x": x_f.tolist(), "max_rel_param_err": float(err_f.max())},
+            "surrogate": {**info_s, "x": x_s.tolist(), "max_rel_param_err": float(err_s.max())},
+            "surrogate_training": info}
+    print(json.dumps(line), flush=True)
+    pr.close()
+    return 0
 
 def C_SIZE_CONTRACT():
     import ctypes

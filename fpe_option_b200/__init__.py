@@ -529,13 +529,26 @@ class Plan:
         self.close()
 
 
-def price_batch(params: np.ndarray, ints: np.ndarray, options: BatchOptions | None = None):
-    """Price n single-strike contracts; returns (prices, status)."""
-    arr, keep = contracts_from_arrays(params, ints)
-    plan = Plan(arr, options, _keep=keep)
-    try:
-        plan.run()
-        p, _, _, _, st = plan.results()
-        return p, st
-    finally:
-        plan.close()
+def price_batch(params: np.ndarray, ints: np.ndarray, options: BatchOptions | None = None,
+                chunk: int = 8192):
+    """Price n single-strike contracts; returns (prices, status).
+
+    Batches larger than ``chunk`` contracts run as consecutive plans of at most
+    ``chunk`` (a plan's device arenas grow with its solves: about 3 MB per
+    solve on a 48 x 24 grid, so 8192 contracts stay near 25 GB)."""
+    params = np.asarray(params)
+    ints = np.asarray(ints)
+    n = len(params)
+    out_p = np.zeros(n)
+    out_s = np.zeros(n, np.int32)
+    for a in range(0, n, max(1, chunk)):
+        b = min(n, a + chunk)
+        arr, keep = contracts_from_arrays(params[a:b], ints[a:b])
+        plan = Plan(arr, options, _keep=keep)
+        try:
+            plan.run()
+            p, _, _, _, st = plan.results()
+            out_p[a:b], out_s[a:b] = p, st
+        finally:
+            plan.close()
+    return out_p, out_s

@@ -70,6 +70,7 @@ EXPORTED = [
     # include/fpe_surrogate.h
     "fpe_mlp_create", "fpe_mlp_destroy", "fpe_mlp_layout", "fpe_mlp_get_params",
     "fpe_mlp_set_params", "fpe_mlp_forward", "fpe_mlp_train_step", "fpe_mlp_gradient",
+    "fpe_mlp_set_lr_schedule",
     "fpe_gemm_bf16",
 ]
 
@@ -143,6 +144,8 @@ def load():
     L.fpe_mlp_train_step.argtypes = [vp, vp, vp, vp, i32, C.c_float, vp, vp]
     L.fpe_mlp_gradient.restype = i32
     L.fpe_mlp_gradient.argtypes = [vp, vp, vp, vp, i32, fp, fp]
+    L.fpe_mlp_set_lr_schedule.restype = i32
+    L.fpe_mlp_set_lr_schedule.argtypes = [vp, fp, i32]
     L.fpe_gemm_bf16.restype = i32
     L.fpe_gemm_bf16.argtypes = [vp, i32, vp, i32, i32, i32, i32, vp, i32, vp, i32, vp]
     L.fpe_price_noalloc.restype = i32

@@ -18,14 +18,19 @@ Two residual back-ends price the whole surface per call:
   noise.
 * ``SurrogateSurface``: the tensor-core MLP ensemble; a Jacobian costs
   microseconds.  Its step is 2 % of the parameter's training range, coarser
-  than the BF16 rounding of the network's inputs.  Quotes the ensemble does
-  not trust (outside its box, or members disagreeing by more than the
-  pricer's tolerance) are priced by the FPE solver inside the loop.
+  than the BF16 rounding of the network's inputs.  Inside the loop quotes
+  outside the training box are priced by the FPE solver; the ensemble mean
+  answers the rest.
 
-``calibrate_with_surrogate`` runs LM on the surrogate, then verifies the fit
-with one batched FPE pricing of the surface and, if the FPE residual is worse
-than the surrogate's by more than ``polish_ratio``, continues LM on the FPE
-solver from there.
+``calibrate_with_surrogate`` runs LM on the surrogate, then polishes on the
+FPE solver: LM whose residuals are FPE prices of the whole surface (every
+quote falls back to the solver, whatever the members' disagreement, which is
+reported) and whose Jacobians are the surrogate's.  Its fixed point
+J_sur^T r_FPE = 0 is the FPE least-squares fit up to a term of second order
+in the Jacobian error times the residual, and each iteration costs one FPE
+pricing of the surface instead of eleven.  ``polish="fpe"`` uses FPE
+Jacobians instead; ``polish="none"`` keeps the surrogate's fit if its FPE
+residual RMS is within ``noise_ratio`` times the quotes' noise level.
 """
 from __future__ import annotations
 
@@ -59,19 +64,23 @@ class LMResult:
 
 def levenberg_marquardt(residual, jacobian, x0, max_iter: int = 50, tol: float = 1e-10,
                         lambda_init: float = 1e-3, lambda_up: float = 10.0,
-                        lambda_down: float = 0.1, xtol: float | None = None) -> LMResult:
+                        lambda_down: float = 0.1, xtol: float | None = None,
+                        ftol: float | None = None, max_rejects: int | None = None) -> LMResult:
     """Reference LM (lm.mojo:29-121).  jacobian(x) returns (r(x), J(x)).
 
-    xtol (not in the reference, off by default) also stops after an accepted
-    step with |delta|_inf <= xtol (|x|_inf + xtol): the test that ends a fit
-    whose residual cannot reach the gradient tolerance (a solver's rounding
-    and step-control noise)."""
+    Stopping tests beyond the reference's gradient test (all off by default),
+    for fits whose residual cannot reach it (quote noise, a solver's rounding
+    and step-control noise): xtol stops after an accepted step with
+    |delta|_inf <= xtol (|x|_inf + xtol); ftol after an accepted step that
+    lowers the cost by less than ftol * cost; max_rejects after that many
+    rejected steps in a row."""
     x = np.array(x0, dtype=np.float64)
     lam = lambda_init
     evals = 0
     hist = []
     it = 0
     cost = np.inf
+    rejects = 0
     for it in range(1, max_iter + 1):
         r, J = jacobian(x)
         evals += 1
@@ -85,13 +94,21 @@ def levenberg_marquardt(residual, jacobian, x0, max_iter: int = 50, tol: float =
         x_new = x + delta
         r_new = residual(x_new)
         evals += 1
-        if float(r_new @ r_new) < cost:
+        c_new = float(r_new @ r_new)
+        if c_new < cost:
             x = x_new
             lam = max(lam * lambda_down, 1e-10)
+            rejects = 0
             if xtol is not None and np.max(np.abs(delta)) <= xtol * (np.max(np.abs(x)) + xtol):
+                break
+            if ftol is not None and cost - c_new < ftol * cost:
+                cost = c_new
                 break
         else:
             lam = lam * lambda_up
+            rejects += 1
+            if max_rejects is not None and rejects >= max_rejects:
+                break
     return LMResult(x=x, iterations=it, residual_evals=evals, cost=cost, history=hist)
 
 
@@ -152,7 +169,11 @@ class _Backend:
         return self.price_sets(np.atleast_2d(x))[0] - self.surface.prices
 
     def jacobian(self, x):
+        """(r(x), J(x)); the pair for the last x is kept, so the repeated call
+        after a rejected LM step (same x) prices nothing."""
         x = np.asarray(x, np.float64)
+        if getattr(self, "_jx", None) is not None and np.array_equal(self._jx, x):
+            return self._jr, self._jJ
         h = self.steps(x)
         xs = [x]
         for j in range(len(x)):
@@ -165,6 +186,7 @@ class _Backend:
         J = np.empty((len(r), len(x)))
         for j in range(len(x)):
             J[:, j] = (p[1 + 2 * j] - p[2 + 2 * j]) / (2.0 * h[j])
+        self._jx, self._jr, self._jJ = x.copy(), r, J
         return r, J
 
 
@@ -223,37 +245,66 @@ class SurrogateSurface(_Backend):
     def price_sets(self, xs):
         t = time.perf_counter()
         P, I = contract_tables(self.surface, np.array([self.project(x) for x in np.atleast_2d(xs)]), self.grid)
-        p, fb = self.pricer.price(P, I)
+        p, fb = self.pricer.price(P, I, gate_disagreement=False)
         self.fallback_quotes += int(fb.sum())
         self.contracts_priced += int(fb.sum())  # FPE solves spent inside the loop
         self.seconds += time.perf_counter() - t
         return p.reshape(len(xs), -1)
 
 
-def calibrate_fpe(surface: Surface, x0, max_iter=40, tol=1e-10, xtol=1e-6, **kw):
+STOP = {"xtol": 1e-6, "ftol": 1e-4, "max_rejects": 6}
+
+
+class HybridSurface:
+    """FPE residuals with the surrogate's Jacobians (see the module notes)."""
+
+    def __init__(self, fpe: FpeSurface, sur: SurrogateSurface):
+        self.fpe, self.sur = fpe, sur
+
+    def residual(self, x):
+        return self.fpe.residual(x)
+
+    def jacobian(self, x):
+        _, J = self.sur.jacobian(x)
+        return self.fpe.residual(x), J
+
+
+def calibrate_fpe(surface: Surface, x0, max_iter=40, tol=1e-10, **kw):
     be = FpeSurface(surface, **kw)
     t = time.perf_counter()
-    res = levenberg_marquardt(be.residual, be.jacobian, x0, max_iter=max_iter, tol=tol, xtol=xtol)
+    res = levenberg_marquardt(be.residual, be.jacobian, x0, max_iter=max_iter, tol=tol, **STOP)
     return clamp(res.x), {"seconds": time.perf_counter() - t, "fpe_contracts": be.contracts_priced,
                           "iterations": res.iterations, "cost": res.cost}
 
 
 def calibrate_with_surrogate(surface: Surface, pricer, x0, max_iter=50, tol=1e-10,
-                             polish_ratio: float = 2.0, polish_iter: int = 10, xtol=1e-6, fpe_kw=None):
+                             polish: str = "hybrid", quote_noise: float | None = None,
+                             noise_ratio: float = 1.5, polish_iter: int = 10, fpe_kw=None):
     """Surrogate-in-loop LM, FPE verification, optional FPE polish."""
     fpe_kw = fpe_kw or {}
     t = time.perf_counter()
     sb = SurrogateSurface(surface, pricer, grid=fpe_kw.get("grid", (48, 24)))
     res = levenberg_marquardt(sb.residual, sb.jacobian, SurrogateSurface.project(x0), max_iter=max_iter,
-                              tol=tol, xtol=1e-4)
+                              tol=tol, xtol=1e-5, ftol=1e-6, max_rejects=6)
     x = clamp(SurrogateSurface.project(res.x))
+    x_sur = x.copy()
     fb = FpeSurface(surface, **fpe_kw)
     r_fpe = fb.residual(x)
     r_sur = sb.residual(x)
+    spread = float(np.max(pricer.last_spread))
+    rms_fpe = float(np.sqrt(np.mean(r_fpe ** 2)))
     polished = False
     it_polish = 0
-    if float(r_fpe @ r_fpe) > polish_ratio * max(float(r_sur @ r_sur), 1e-30):
-        pol = levenberg_marquardt(fb.residual, fb.jacobian, x, max_iter=polish_iter, tol=tol, xtol=xtol)
+    if polish == "hybrid":
+        hb = HybridSurface(fb, sb)
+        # near-Gauss-Newton steps: the fit starts close to the optimum
+        pol = levenberg_marquardt(hb.residual, hb.jacobian, x, max_iter=polish_iter, tol=tol,
+                                  lambda_init=1e-9, **STOP)
+        x = clamp(pol.x)
+        polished = True
+        it_polish = pol.iterations
+    elif polish == "fpe" or (polish == "none" and (quote_noise is None or rms_fpe > noise_ratio * quote_noise)):
+        pol = levenberg_marquardt(fb.residual, fb.jacobian, x, max_iter=polish_iter, tol=tol, **STOP)
         x = clamp(pol.x)
         polished = True
         it_polish = pol.iterations
@@ -261,4 +312,6 @@ def calibrate_with_surrogate(surface: Surface, pricer, x0, max_iter=50, tol=1e-1
                "fpe_contracts": fb.contracts_priced + sb.contracts_priced,
                "surrogate_iterations": res.iterations, "polished": polished,
                "polish_iterations": it_polish, "fallback_quotes": sb.fallback_quotes,
-               "fpe_rms_at_surrogate_fit": float(np.sqrt(np.mean(r_fpe ** 2)))}
+               "max_disagreement_at_fit": spread, "x_surrogate_fit": x_sur.tolist(),
+               "fpe_rms_at_surrogate_fit": rms_fpe,
+               "surrogate_rms_at_fit": float(np.sqrt(np.mean(r_sur ** 2)))}

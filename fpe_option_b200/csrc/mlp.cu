@@ -20,6 +20,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -135,6 +136,9 @@ struct GemmParams {
   int ldcb;
   bf16* CbT;  // transposed (N x M)
   int ldcbt;
+  int tn;      // N tile width (16..256, a multiple of 16)
+  int ksplit;  // K slices (grid z); > 1 only with EPI_F32 + atomic
+  int atomic;  // EPI_F32: accumulate into Cf with atomicAdd (Cf zeroed by the caller)
   int* err;
 };
 
@@ -155,8 +159,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ unsigned long long bar[2];
   __shared__ uint32_t tmem_slot;
-  const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * kTileN;
-  const int Nt = min(kTileN, P.N - n0);
+  const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * P.tn;
+  const int Nt = min(P.tn, P.N - n0);
+  // K slice of this CTA (split-K): whole 64-wide chunks
+  const int kslice = ((P.K + P.ksplit - 1) / P.ksplit + kChunkK - 1) / kChunkK * kChunkK;
+  const int kbeg = blockIdx.z * kslice, kend = min(P.K, kbeg + kslice);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint32_t ncols = 32;
   while (int(ncols) < Nt) ncols <<= 1;
@@ -174,16 +181,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
 
-  const int nchunk = (P.K + kChunkK - 1) / kChunkK;
+  const int nchunk = kend > kbeg ? (kend - kbeg + kChunkK - 1) / kChunkK : 0;
   const uint32_t idesc = umma_idesc_bf16(kTileM, Nt);
   uint32_t phase = 0;
   bool ok = true;
   auto load = [&](int c, int b) {
-    const int k0 = c * kChunkK, kc = min(kChunkK, P.K - k0);
+    const int k0 = kbeg + c * kChunkK, kc = min(kChunkK, kend - k0);
     stage_kmajor(bufA[b], P.A, P.lda, m0, kTileM, k0, kc);
     stage_kmajor(bufB[b], P.B, P.ldb, n0, Nt, k0, kc);
   };
-  load(0, 0);
+  if (nchunk > 0) load(0, 0);
   fence_proxy_async_smem();
   __syncthreads();
   for (int c = 0; c < nchunk; ++c) {
@@ -199,7 +206,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
     }
     if (tid == 0 && ok) {
       tc_fence_after();
-      const int k0 = c * kChunkK, kc = min(kChunkK, P.K - k0), k8n = kc >> 3;
+      const int k0 = kbeg + c * kChunkK, kc = min(kChunkK, kend - k0), k8n = kc >> 3;
       const uint32_t sa = smem_u32(bufA[b]), sb = smem_u32(bufB[b]);
       for (int s = 0; s < (kc >> 4); ++s) {
         const uint64_t ad = umma_desc(sa + 256u * s, 128u, uint32_t(k8n) * 128u);
@@ -212,7 +219,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
     fence_proxy_async_smem();
     __syncthreads();
   }
-  {
+  if (nchunk > 0) {
     const int bl = (nchunk - 1) & 1;
     if (mbar_wait_bounded(&bar[bl], (phase >> bl) & 1u, kBulkWaitLimit)) {
       phase ^= 1u << bl;
@@ -222,7 +229,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
     tc_fence_after();
   }
   ok = __syncthreads_and(ok ? 1 : 0) != 0;
-  if (ok) {
+  if (ok && nchunk > 0) {
     const int r = 32 * warp + lane;
     const int gm = m0 + r;
     const uint32_t trow = tmem + (uint32_t(32 * warp) << 16);
@@ -248,7 +255,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
           v[j] *= s * (1.0f + z * (1.0f - s));
         }
       }
-      if (P.Cf) {
+      if (P.Cf && P.atomic) {
+        float* d = P.Cf + size_t(gm) * P.ldcf + gn;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) atomicAdd(d + j, v[j]);
+      } else if (P.Cf) {
         float4* d = reinterpret_cast<float4*>(P.Cf + size_t(gm) * P.ldcf + gn);
 #pragma unroll
         for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
@@ -271,7 +282,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
         }
       }
     }
-  } else if (tid == 0 && P.err) {
+  } else if (!ok && tid == 0 && P.err) {
     atomicExch(P.err, 1);
   }
   tc_fence_before();
@@ -385,11 +396,25 @@ __global__ void k_sum(const float* __restrict__ x, int n, float* __restrict__ ou
   }
 }
 
+// Step counter and hyper-parameters of one Adam step, on the device so that
+// a captured training step replays correctly: t = ++step, lr = lr_arg, or
+// (lr_arg < 0) the schedule entry of step t; hyper = {lr, 1 - b1^t, 1 - b2^t}.
+__global__ void k_adam_prologue(int* __restrict__ step, const float* __restrict__ table, int len, float lr_arg,
+                                float b1, float b2, float* __restrict__ hyper) {
+  const int t = ++step[0];
+  float lr = lr_arg;
+  if (lr_arg < 0.0f) lr = (table && len > 0) ? table[min(t - 1, len - 1)] : 0.0f;
+  hyper[0] = lr;
+  hyper[1] = 1.0f - powf(b1, float(t));
+  hyper[2] = 1.0f - powf(b2, float(t));
+}
+
 // Adam (reference src/nn/adam.mojo:31-64): m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2,
 // theta -= lr * (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps).
 __global__ void k_adam(float* __restrict__ theta, const float* __restrict__ g, float* __restrict__ m,
-                       float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps, float c1,
-                       float c2) {
+                       float* __restrict__ v, int64_t n, const float* __restrict__ hyper, float b1, float b2,
+                       float eps) {
+  const float lr = hyper[0], c1 = hyper[1], c2 = hyper[2];
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     const float gi = g[i];
     const float mi = b1 * m[i] + (1.0f - b1) * gi;
@@ -460,7 +485,9 @@ int launch_gemm(const fpe::mlp::GemmParams& P, cudaStream_t s) {
   if ((reinterpret_cast<uintptr_t>(P.A) | reinterpret_cast<uintptr_t>(P.B)) & 15) return -1;
   if (P.Cf && (P.ldcf % 4 || (reinterpret_cast<uintptr_t>(P.Cf) & 15))) return -1;
   if (P.Cb && (P.ldcb % 8 || (reinterpret_cast<uintptr_t>(P.Cb) & 15))) return -1;
-  const dim3 grid(P.M / kTileM, (P.N + kTileN - 1) / kTileN);
+  if (P.tn < 16 || P.tn > kTileN || P.tn % 16 || P.ksplit < 1) return -1;
+  if (P.ksplit > 1 && !(P.epi == EPI_F32 && P.atomic && !P.bias && !P.act && !P.Cb && !P.CbT)) return -1;
+  const dim3 grid(P.M / kTileM, (P.N + P.tn - 1) / P.tn, P.ksplit);
   k_gemm_bf16_tc<<<grid, kThreads, kSmemBytes, s>>>(P);
   MK(cudaGetLastError());
   return 0;
@@ -477,6 +504,10 @@ fpe::mlp::GemmParams gp(const bf16* A, int lda, const bf16* B, int ldb, int M, i
   P.K = K;
   P.epi = epi;
   P.err = err;
+  // narrower N tiles when the row tiles alone would leave most SMs idle
+  P.tn = (M / fpe::mlp::kTileM < 74 && N >= 256) ? 128 : std::min(N, fpe::mlp::kTileN);
+  if (P.tn % 16) P.tn = fpe::mlp::kTileN;
+  P.ksplit = 1;
   return P;
 }
 
@@ -508,7 +539,10 @@ struct FpeMlp {
   bf16 *dZb[2] = {nullptr, nullptr}, *dZbT[2] = {nullptr, nullptr};
   float *yhat = nullptr, *dy = nullptr, *loss = nullptr;
   int* err = nullptr;
-  int64_t step = 0;
+  int* step = nullptr;          // Adam step counter (device)
+  float* hyper = nullptr;       // {lr, 1 - b1^t, 1 - b2^t} of the current step (device)
+  float* lr_table = nullptr;    // learning-rate schedule (device), lr_len entries
+  int lr_len = 0;
   std::vector<void*> allocs;
 
   int in_of(int l) const { return l == 0 ? in_pad : hidden; }
@@ -591,6 +625,12 @@ int mlp_backward(FpeMlp* M, const float* x, const float* y, const float* w, int 
     GemmParams P = gp(M->dZbT[cur], R, Bt, R, Hd, in, R, EPI_F32, M->err);
     P.Cf = M->grad + M->off_w[l];
     P.ldcf = in;
+    // the batch is the reduction dimension: split it so that the few row
+    // tiles (hidden / 128) still spread over the SMs, accumulating atomically
+    P.tn = std::min(in, fpe::mlp::kTileN);
+    P.ksplit = std::max(1, std::min(64, R / 128));
+    P.atomic = 1;
+    MK(cudaMemsetAsync(P.Cf, 0, size_t(Hd) * in * sizeof(float), s));
     if (launch_gemm(P, s)) return -1;
     k_colsum<float><<<(Hd + 31) / 32, 256, 0, s>>>(M->dZ[cur], Hd, R, Hd, nullptr, M->grad + M->off_b[l]);
     if (l > 0) {
@@ -677,7 +717,8 @@ FpeMlp* fpe_mlp_create(int32_t n_in, int32_t hidden, int32_t layers, int32_t max
   for (int k = 0; k < 2 && !bad; ++k)
     bad = M->alloc(&M->dZ[k], R * hidden) || M->alloc(&M->dZb[k], R * hidden) || M->alloc(&M->dZbT[k], R * hidden);
   bad = bad || M->alloc(&M->X, R * M->in_pad) || M->alloc(&M->XT, R * M->in_pad) || M->alloc(&M->yhat, R) ||
-        M->alloc(&M->dy, R) || M->alloc(&M->loss, 1) || M->alloc(&M->err, 1);
+        M->alloc(&M->dy, R) || M->alloc(&M->loss, 1) || M->alloc(&M->err, 1) || M->alloc(&M->step, 1) ||
+        M->alloc(&M->hyper, 4);
   if (bad || cudaMemcpy(M->theta, h.data(), size_t(o) * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
       mlp_cast_all(M, mctx().stream) || cudaStreamSynchronize(mctx().stream) != cudaSuccess) {
     delete M;
@@ -717,7 +758,7 @@ int32_t fpe_mlp_set_params(FpeMlp* M, const float* in, int64_t n) {
   MK(cudaMemcpy(M->theta, in, size_t(n) * sizeof(float), cudaMemcpyHostToDevice));
   MK(cudaMemset(M->m, 0, size_t(n) * sizeof(float)));
   MK(cudaMemset(M->v, 0, size_t(n) * sizeof(float)));
-  M->step = 0;
+  MK(cudaMemset(M->step, 0, sizeof(int)));
   if (mlp_cast_all(M, s)) return -1;
   MK(cudaStreamSynchronize(s));
   return 0;
@@ -744,13 +785,30 @@ int32_t fpe_mlp_train_step(FpeMlp* M, const float* x, const float* y, const floa
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : mctx().stream;
   if (mlp_backward(M, x, y, w, n, s)) return -1;
   if (loss_dev) MK(cudaMemcpyAsync(loss_dev, M->loss, sizeof(float), cudaMemcpyDeviceToDevice, s));
-  M->step += 1;
   const float b1 = 0.9f, b2 = 0.999f;
-  const float c1 = 1.0f - std::pow(b1, float(M->step)), c2 = 1.0f - std::pow(b2, float(M->step));
-  fpe::mlp::k_adam<<<grid_for(M->n_params), 256, 0, s>>>(M->theta, M->grad, M->m, M->v, M->n_params, lr, b1, b2,
-                                                          1e-8f, c1, c2);
+  fpe::mlp::k_adam_prologue<<<1, 1, 0, s>>>(M->step, M->lr_table, M->lr_len, lr, b1, b2, M->hyper);
+  fpe::mlp::k_adam<<<grid_for(M->n_params), 256, 0, s>>>(M->theta, M->grad, M->m, M->v, M->n_params, M->hyper,
+                                                          b1, b2, 1e-8f);
   MK(cudaGetLastError());
   return mlp_cast_all(M, s);
+}
+
+int32_t fpe_mlp_set_lr_schedule(FpeMlp* M, const float* host_table, int32_t n) {
+  if (!M || n < 0 || (n > 0 && !host_table)) return -1;
+  MK(cudaStreamSynchronize(mctx().stream));
+  if (M->lr_table) {
+    cudaFree(M->lr_table);
+    for (auto& p : M->allocs)
+      if (p == M->lr_table) p = nullptr;
+    M->lr_table = nullptr;
+    M->lr_len = 0;
+  }
+  if (n > 0) {
+    if (M->alloc(&M->lr_table, size_t(n))) return -1;
+    MK(cudaMemcpy(M->lr_table, host_table, size_t(n) * sizeof(float), cudaMemcpyHostToDevice));
+    M->lr_len = n;
+  }
+  return 0;
 }
 
 int32_t fpe_mlp_gradient(FpeMlp* M, const float* x, const float* y, const float* w, int32_t n, float* grad_host,

@@ -53,6 +53,12 @@ class Mlp:
                 self._h, th.ctypes.data_as(C.POINTER(C.c_float)), self.n_params):
             raise RuntimeError("fpe_mlp_set_params failed")
 
+    def set_lr_schedule(self, table) -> None:
+        """Per-step learning rates used by train steps given lr < 0."""
+        t = np.ascontiguousarray(table, dtype=np.float32)
+        if self._L.fpe_mlp_set_lr_schedule(self._h, t.ctypes.data_as(C.POINTER(C.c_float)), int(t.size)):
+            raise RuntimeError("fpe_mlp_set_lr_schedule failed")
+
     # -- device-tensor entry points --------------------------------------------
     def _stream(self, stream):
         """The CUDA stream for a call: the given one, else torch's current stream
@@ -138,11 +144,24 @@ BOX_HI = np.array([3.0, 0.15, 0.8, 0.0, 0.2, 0.05, 2.0, 1.3, 1.4])
 # option types the surrogate covers: European call/put, down-and-out/in calls,
 # up-and-out/in puts
 SURROGATE_TYPES = (8, 9, 2, 0, 7, 5)
-# The network predicts y = log(price / S0 + LOG_EPS): squared error in y is a
-# relative-price error floored at LOG_EPS S0, and the BF16 rounding of the
-# activations (about 2^-9 relative) becomes a uniform relative price error
-# instead of an absolute one that would swamp small prices.
+# The network predicts y = log(v / S0 + LOG_EPS), v the option's value above
+# its discounted intrinsic value for Europeans (price - (S0 - K e^{-rT})+ for
+# calls, price - (K e^{-rT} - S0)+ for puts) and the price itself for barrier
+# options: squared error in y is a relative error of the part of the price
+# that depends on the model, floored at LOG_EPS S0, and the BF16 rounding of
+# the activations (about 2^-9 relative) becomes a relative error of that part
+# instead of an absolute one that would swamp small or deep in-the-money prices.
 LOG_EPS = 1e-3
+
+
+def intrinsic(params, ints) -> np.ndarray:
+    """Discounted intrinsic value of European quotes (zero for other types)."""
+    P = np.asarray(params, np.float64)
+    t = np.asarray(ints)[:, 2]
+    fwd = P[:, 8] * np.exp(-P[:, 4] * P[:, 5])
+    call = np.maximum(P[:, 6] - fwd, 0.0)
+    put = np.maximum(fwd - P[:, 6], 0.0)
+    return np.where(t == 8, call, np.where(t == 9, put, 0.0))
 
 
 def encode(params: np.ndarray, ints: np.ndarray):
@@ -235,6 +254,8 @@ class SurrogatePricer:
         self.members = [Mlp(12, c.hidden, c.layers, max(c.batch, 128), seed=c.seed + 101 * k)
                         for k in range(c.members)]
         self._torch = _torch()
+        # the networks learn standardised targets (y - mu) / sd, fixed at fit()
+        self.mu, self.sd = 0.0, 1.0
 
     # -- data ---------------------------------------------------------------------
     def fpe_prices(self, params, ints) -> np.ndarray:
@@ -247,52 +268,67 @@ class SurrogatePricer:
         return p
 
     @staticmethod
-    def targets(params, prices):
-        """Training targets log(price / S0 + LOG_EPS) and unit weights."""
-        y = np.asarray(prices, np.float64) / np.asarray(params, np.float64)[:, 6]
-        y = np.log(np.maximum(y, 0.0) + LOG_EPS)
+    def targets(params, ints, prices):
+        """Training targets log(v / S0 + LOG_EPS) (v: see LOG_EPS) and unit weights."""
+        P = np.asarray(params, np.float64)
+        v = (np.asarray(prices, np.float64) - intrinsic(P, ints)) / P[:, 6]
+        y = np.log(np.maximum(v, 0.0) + LOG_EPS)
         return y, np.ones_like(y)
 
     @staticmethod
-    def to_price(y, S0):
-        return np.asarray(S0) * (np.exp(np.asarray(y, np.float64)) - LOG_EPS)
+    def to_price(y, params, ints):
+        P = np.asarray(params, np.float64)
+        return P[:, 6] * (np.exp(np.asarray(y, np.float64)) - LOG_EPS) + intrinsic(P, ints)
 
     # -- training -------------------------------------------------------------------
     def fit(self, params, ints, prices, epochs: int | None = None, log=None) -> list[float]:
-        """Adam on the relative squared error; returns the last epoch loss per member."""
+        """Adam on the squared error of the standardised log-price targets;
+        returns the last epoch's mean loss per member.
+
+        One epoch -- the batch gathers and the training steps of every batch --
+        is captured once as a CUDA graph per member and replayed each epoch with
+        a fresh permutation; the cosine learning-rate schedule is read on the
+        device by the step counter, so every replay trains with the right rate."""
         torch = self._torch
         c = self.config
         epochs = c.epochs if epochs is None else epochs
         x, _ = encode(params, ints)
-        y, w = self.targets(params, prices)
+        y, w = self.targets(params, ints, prices)
+        self.mu, self.sd = float(y.mean()), float(max(y.std(), 1e-12))
+        y = (y - self.mu) / self.sd
         tx = torch.as_tensor(x, device="cuda")
         ty = torch.as_tensor(y.astype(np.float32), device="cuda")
         tw = torch.as_tensor(w.astype(np.float32), device="cuda")
         n = len(x)
         bs = min(c.batch, n)
-        steps = max(1, epochs * (n // bs))
+        nb = n // bs
+        steps = max(1, epochs * nb)
+        sched = 0.5 * c.lr * (1.0 + np.cos(np.pi * np.arange(steps) / steps))
         losses = []
         for k, net in enumerate(self.members):
+            net.set_lr_schedule(sched)
             gen = torch.Generator(device="cuda")
             gen.manual_seed(c.seed * 7919 + k)
+            perm = torch.zeros(nb * bs, dtype=torch.long, device="cuda")
             loss = torch.zeros(1, device="cuda")
-            step = 0
-            for ep in range(epochs):
-                perm = torch.randperm(n, device="cuda", generator=gen)
-                acc = torch.zeros(1, device="cuda")
-                nb = 0
-                for s in range(0, n - bs + 1, bs):
-                    idx = perm[s:s + bs]
-                    lr = 0.5 * c.lr * (1.0 + np.cos(np.pi * step / steps))
-                    step += 1
-                    net.train_step_dev(tx[idx].contiguous(), ty[idx].contiguous(), tw[idx].contiguous(),
-                                       lr, loss)
+            acc = torch.zeros(1, device="cuda")
+            torch.cuda.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                acc.zero_()
+                for b in range(nb):
+                    idx = perm[b * bs:(b + 1) * bs]
+                    net.train_step_dev(tx.index_select(0, idx), ty.index_select(0, idx),
+                                       tw.index_select(0, idx), -1.0, loss)
                     acc += loss
-                    nb += 1
+            for ep in range(epochs):
+                perm.copy_(torch.randperm(n, device="cuda", generator=gen)[:nb * bs])
+                graph.replay()
                 if log is not None and (ep + 1) % max(1, epochs // 5) == 0:
-                    log(f"member {k} epoch {ep + 1}: loss {float(acc.item()) / max(nb, 1):.3e}")
-            losses.append(float(acc.item()) / max(nb, 1))
-        torch.cuda.synchronize()
+                    log(f"member {k} epoch {ep + 1}: loss {float(acc.item()) / nb:.3e}")
+            torch.cuda.synchronize()
+            losses.append(float(acc.item()) / nb)
+            del graph
         return losses
 
     # -- inference --------------------------------------------------------------------
@@ -305,23 +341,41 @@ class SurrogatePricer:
         outs = torch.empty((len(self.members), n), device="cuda")
         for k, net in enumerate(self.members):
             net.forward_dev(x_dev, outs[k])
-        mean = outs.mean(0)
-        spread = outs.max(0).values - outs.min(0).values
+        mean = outs.mean(0) * self.sd + self.mu
+        spread = (outs.max(0).values - outs.min(0).values) * self.sd
         return mean, spread
 
-    def price(self, params, ints):
-        """(prices, from_fpe mask): the surrogate where it is trusted, FPE elsewhere."""
+    def price(self, params, ints, gate_disagreement: bool = True):
+        """(prices, from_fpe mask): the surrogate where it is trusted, FPE elsewhere.
+        Trusted = inside the training box and, with gate_disagreement, members
+        agreeing to disagreement_tol."""
         torch = self._torch
         P = np.asarray(params, np.float64)
         x, in_box = encode(P, ints)
         mean, spread = self.predict_features(torch.as_tensor(x, device="cuda"))
         y = mean.cpu().numpy().astype(np.float64)
-        ok = in_box & (spread.cpu().numpy() <= self.config.disagreement_tol)
-        prices = self.to_price(y, P[:, 6])
+        self.last_spread = spread.cpu().numpy()
+        ok = in_box & ((self.last_spread <= self.config.disagreement_tol) | (not gate_disagreement))
+        prices = self.to_price(y, P, ints)
         fb = ~ok
         if np.any(fb):
             prices[fb] = self.fpe_prices(P[fb], np.asarray(ints)[fb])
         return prices, fb
+
+    def save(self, path: str) -> None:
+        """Parameters of every member and the target standardisation (npz)."""
+        c = self.config
+        np.savez(path, mu=self.mu, sd=self.sd, hidden=c.hidden, layers=c.layers,
+                 members=np.stack([m.get_params() for m in self.members]))
+
+    def load(self, path: str) -> None:
+        d = np.load(path)
+        if int(d["hidden"]) != self.config.hidden or int(d["layers"]) != self.config.layers or \
+                len(d["members"]) != len(self.members):
+            raise ValueError("saved surrogate does not match this configuration")
+        for m, th in zip(self.members, d["members"]):
+            m.set_params(th)
+        self.mu, self.sd = float(d["mu"]), float(d["sd"])
 
     def close(self):
         for m in self.members:

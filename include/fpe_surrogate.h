@@ -48,10 +48,18 @@ extern int32_t fpe_mlp_forward(FpeMlp* mlp, const float* x_dev, int32_t n, float
 /** One Adam step (learning rate lr, beta1 0.9, beta2 0.999, eps 1e-8) on the
  *  weighted squared error  sum_i w_i (y_hat_i - y_i)^2 / n  over n <= max_rows
  *  rows; w_dev may be NULL (weights 1).  loss_dev (optional, device float)
- *  receives the loss before the step. */
+ *  receives the loss before the step.  lr < 0 takes the rate of the current
+ *  step from the schedule set by fpe_mlp_set_lr_schedule.  The step counter
+ *  and bias corrections live on the device and the call makes no host
+ *  synchronisation, so a sequence of steps can be captured in a CUDA graph on
+ *  a caller's stream and replayed. */
 extern int32_t fpe_mlp_train_step(FpeMlp* mlp, const float* x_dev, const float* y_dev,
                                   const float* w_dev, int32_t n, float lr, float* loss_dev,
                                   void* cuda_stream);
+
+/** Learning-rate schedule: entry t - 1 is the rate of Adam step t (the last
+ *  entry repeats); n = 0 clears it.  Copied to the device. */
+extern int32_t fpe_mlp_set_lr_schedule(FpeMlp* mlp, const float* host_table, int32_t n);
 
 /** Gradient of the same loss at the current parameters, copied to
  *  grad_host[n_params] (no update); *loss_host receives the loss. */
