@@ -187,6 +187,7 @@ def main():
                     help="batch: the batched FPE pricing line (default); surrogate / calibration: "
                          "the learned part's measurements")
     ap.add_argument("--train", type=int, default=65536, help="surrogate training prices")
+    ap.add_argument("--surfaces", type=int, default=5, help="calibration: seeded surfaces")
     ap.add_argument("--surrogate-file", default=None,
                     help="calibration: load a trained European ensemble (npz) instead of training; "
                          "if the file does not exist, train and save it there")
@@ -458,32 +459,48 @@ def run_learned_workload(args):
         info["epochs"], info["batch"] = ep, bs
         if args.surrogate_file:
             pr.save(args.surrogate_file)
-    rng = np.random.default_rng(4242 + args.seed)
-    truth = np.array([rng.uniform(0.8, 2.5), rng.uniform(0.03, 0.12), rng.uniform(0.2, 0.7),
-                      rng.uniform(-0.8, -0.2), rng.uniform(0.03, 0.15)])
-    surf = Surface.grid(100.0, 0.02, np.linspace(0.7, 1.3, 15), np.linspace(0.1, 2.0, 8))
-    P, I = contract_tables(surf, truth, SUR_GRID)
-    p, st = fpe.price_batch(P, I, fpe.BatchOptions(disc=1, precision=0, rtol=1e-9, atol=1e-11,
-                                                   complex_solve=2, radau_constants=2))
-    assert (st == 0).all()
-    surf.prices = p + rng.normal(0.0, 1e-4 * 100.0, p.shape)
-    x0 = np.array([1.5, 0.08, 0.45, -0.45, 0.08])
+    surfaces = []
     kw = {"grid": SUR_GRID}
-    x_f, info_f = calibrate_fpe(surf, x0, **kw)
-    x_s, info_s = calibrate_with_surrogate(surf, pr, x0, max_iter=50, polish_iter=30, fpe_kw=kw,
-                                           quote_noise=1e-4 * 100.0)
-    err_f = np.abs(x_f - truth) / np.abs(truth)
-    err_s = np.abs(x_s - truth) / np.abs(truth)
+    noise = 1e-4 * 100.0
+    res = {"fpe_only": [], "surrogate": [], "hybrid": []}
+    for k in range(args.surfaces):
+        rng = np.random.default_rng(4242 + 97 * k + args.seed)
+        truth = np.array([rng.uniform(0.8, 2.5), rng.uniform(0.03, 0.12), rng.uniform(0.2, 0.7),
+                          rng.uniform(-0.8, -0.2), rng.uniform(0.03, 0.15)])
+        surf = Surface.grid(100.0, 0.02, np.linspace(0.7, 1.3, 15), np.linspace(0.1, 2.0, 8))
+        P, I = contract_tables(surf, truth, SUR_GRID)
+        p, st = fpe.price_batch(P, I, fpe.BatchOptions(disc=1, precision=0, rtol=1e-9, atol=1e-11,
+                                                       complex_solve=2, radau_constants=2))
+        assert (st == 0).all()
+        surf.prices = p + rng.normal(0.0, noise, p.shape)
+        x0 = np.array([1.5, 0.08, 0.45, -0.45, 0.08])
+        x_f, i_f = calibrate_fpe(surf, x0, **kw)
+        x_s, i_s = calibrate_with_surrogate(surf, pr, x0, max_iter=50, polish="none", quote_noise=noise,
+                                            polish_iter=30, fpe_kw=kw)
+        x_h, i_h = calibrate_with_surrogate(surf, pr, x0, max_iter=50, polish="hybrid", polish_iter=30, fpe_kw=kw)
+        for name, x, inf in (("fpe_only", x_f, i_f), ("surrogate", x_s, i_s), ("hybrid", x_h, i_h)):
+            inf = dict(inf)
+            inf["max_rel_param_err"] = float(np.max(np.abs(x - truth) / np.abs(truth)))
+            inf["x"] = x.tolist()
+            res[name].append(inf)
+        surfaces.append(truth.tolist())
+    summ = {}
+    for name, lst in res.items():
+        summ[name] = {"seconds_total": float(sum(d["seconds"] for d in lst)),
+                      "fpe_contracts_total": int(sum(d["fpe_contracts"] for d in lst)),
+                      "mean_max_rel_param_err": float(np.mean([d["max_rel_param_err"] for d in lst])),
+                      "median_max_rel_param_err": float(np.median([d["max_rel_param_err"] for d in lst]))}
     line = {"metric": "Heston calibration wall time: surrogate-in-loop vs FPE-only (same GPU)",
-            "value": info_f["seconds"] / info_s["seconds"], "unit": "x speed-up", "n_gpus": 1,
-            "higher_is_better": True, "data": "synthetic", "workload": "calibration",
-            "config": {"workload": "15 strikes (K/S0 0.7-1.3) x 8 maturities (0.1-2.0), European calls, "
-                                   "FP64 FPE surface of a seeded parameter set + N(0, 1e-4 S0) noise, "
-                                   f"{SUR_GRID[0]}x{SUR_GRID[1]} grids"},
-            "truth": truth.tolist(),
-            "fpe_only": {**info_f, "x": x_f.tolist(), "max_rel_param_err": float(err_f.max())},
-            "surrogate": {**info_s, "x": x_s.tolist(), "max_rel_param_err": float(err_s.max())},
-            "surrogate_training": info}
+            "value": summ["fpe_only"]["seconds_total"] / summ["surrogate"]["seconds_total"],
+            "unit": "x speed-up", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "workload": "calibration",
+            "config": {"workload": f"{args.surfaces} seeded surfaces of 15 strikes (K/S0 0.7-1.3) x 8 maturities "
+                                   "(0.1-2.0), European calls, FP64 FPE prices + N(0, 1e-4 S0) noise, "
+                                   f"{SUR_GRID[0]}x{SUR_GRID[1]} grids; surrogate: LM on the ensemble, one FPE "
+                                   "verification, FPE polish only if the FPE residual RMS exceeds 1.5x the noise; "
+                                   "hybrid: FPE residuals with surrogate Jacobians"},
+            "summary": summ, "hybrid_speedup": summ["fpe_only"]["seconds_total"] / summ["hybrid"]["seconds_total"],
+            "truths": surfaces, "runs": res, "surrogate_training": info}
     print(json.dumps(line), flush=True)
     pr.close()
     return 0

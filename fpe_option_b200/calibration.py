@@ -242,6 +242,16 @@ class SurrogateSurface(_Backend):
     def steps(self, x):
         return self.frac_step * self._RANGE
 
+    def jacobian(self, x):
+        """As the base class, with the difference stencil moved inside the box
+        where x lies on or near its edge (a projected stencil would flatten
+        the column)."""
+        h = self.steps(x)
+        c = np.clip(np.asarray(x, np.float64), self.LO + h, self.HI - h)
+        r = self.residual(x)
+        _, J = super().jacobian(c)
+        return r, J
+
     def price_sets(self, xs):
         t = time.perf_counter()
         P, I = contract_tables(self.surface, np.array([self.project(x) for x in np.atleast_2d(xs)]), self.grid)
