@@ -183,7 +183,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-sample", type=int, default=8,
                     help="contracts timed on the plain one-solve-per-launch FP64 path")
-    ap.add_argument("--workload", default="batch", choices=["batch", "surrogate", "calibration"],
+    ap.add_argument("--workload", default="batch", choices=["batch", "barrier", "surrogate", "calibration"],
                     help="batch: the batched FPE pricing line (default); surrogate / calibration: "
                          "the learned part's measurements")
     ap.add_argument("--train", type=int, default=65536, help="surrogate training prices")
@@ -198,6 +198,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "barrier":
+        return run_barrier_workload(args)
     if args.workload != "batch":
         return run_learned_workload(args)
 
@@ -503,6 +505,78 @@ def run_learned_workload(args):
             "truths": surfaces, "runs": res, "surrogate_training": info}
     print(json.dumps(line), flush=True)
     pr.close()
+    return 0
+
+
+def make_barrier_batch(n: int, seed: int):
+    """Knock-in contracts on the batched-workload parameter draws: down-and-in
+    calls with B/S0 ~ U[0.6, 0.95] and up-and-in puts with B/S0 ~ U[1.05, 1.4]
+    (half each), K/S0 ~ U[0.8, 1.2], grids n_s in {48, 64, 96} x n_v in
+    {24, 32, 48}; each costs two solves (in-out parity), one of them on the
+    domain truncated at B."""
+    P, I = make_batch(n, seed)
+    rng = np.random.default_rng(seed + 7)
+    down = np.arange(n) % 2 == 0
+    P[:, 9] = np.where(down, 100.0 * rng.uniform(0.6, 0.95, n), 100.0 * rng.uniform(1.05, 1.4, n))
+    I[:, 0] = rng.choice([48, 64, 96], n)
+    I[:, 1] = rng.choice([24, 32, 48], n)
+    I[:, 2] = np.where(down, 0, 5)
+    return P, I
+
+
+def run_barrier_workload(args):
+    import torch
+
+    import fpe_option_b200 as fpe
+    from fpe_option_b200 import build
+
+    build.build_library()
+    if not fpe.is_available():
+        raise RuntimeError("CUDA engine unavailable")
+    nc = 1024
+    P, I = make_barrier_batch(nc, args.seed)
+    opts = fpe.BatchOptions(disc=1, precision=args.precision, rtol=args.rtol, atol=args.rtol * 1e-2,
+                            complex_solve=2, radau_constants=2)
+    arr, keep = fpe.contracts_from_arrays(P, I)
+    plan = fpe.Plan(arr, opts, _keep=keep)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sptr = stream.cuda_stream
+    for _ in range(max(args.warmup, 3)):
+        plan.run(sptr)
+    torch.cuda.synchronize()
+    p_out, _, _, _, st = plan.results()
+    ktimes = plan.kernel_times(sptr)
+    stats = plan.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.run(sptr)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # accuracy on a subsample against FP64 at a tight tolerance
+    sub = np.arange(0, nc, nc // 64)
+    ref, st_ref = fpe.price_batch(P[sub], I[sub], fpe.BatchOptions(
+        disc=1, precision=0, rtol=1e-10, atol=1e-12, complex_solve=2, radau_constants=2))
+    floor = 1e-6 * 100.0
+    rel = np.abs(p_out[sub] - ref) / np.maximum(np.abs(ref), floor)
+    line = {"metric": "FPE knock-in prices/sec on 1 B200 (in-out parity, two solves each)",
+            "value": nc / (ms / 1000.0), "unit": "prices/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "dtype": "f32-factors/f64" if args.precision == 1 else "f64", "data": "synthetic",
+            "workload": "barrier",
+            "config": {"workload": f"{nc} knock-in contracts ({stats['solves']} solves), grids 48-96 x 24-48, "
+                                   "one launch sequence", "rtol": args.rtol,
+                       "max_rel_err_vs_fp64_subsample": float(rel.max()), "subsample": int(len(sub)),
+                       "err_floor": floor, "status_ok": bool((st == 0).all() and (st_ref == 0).all())},
+            "gpu_launches": 5 * args.steps,
+            "kernel_ms": {"setup": ktimes[0], "galerkin": ktimes[1], "ic": ktimes[2], "radau": ktimes[3],
+                          "payoff": ktimes[4]},
+            "solver": {k: int(v) for k, v in stats.items()}, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    plan.close()
     return 0
 
 def C_SIZE_CONTRACT():

@@ -231,7 +231,8 @@ struct FpePlan {
 
 static int plan_layout(FpePlan* P, int esz) {
   int64_t od = 0, oi = 0, of = 0, ot = 0;
-  size_t smem_max = 0, smem_base_max = 0;
+  size_t smem_fit_max = 0, smem_base_max = 0;
+  const size_t optin = size_t(ctx().smem_optin > 0 ? ctx().smem_optin : 232448);
   const int cplx = P->o.complex_mode;
   for (auto& d : P->descs) {
     d.off_d = od;
@@ -252,22 +253,26 @@ static int plan_layout(FpePlan* P, int esz) {
                 (cplx ? size_t(fpe_fac_scratch_elems(nv)) * 2 * esz + 16 : 0);
     (void)ebytes;
     smem_base_max = std::max(smem_base_max, base);
-    smem_max = std::max(smem_max, sm);
+    if (sm <= optin) smem_fit_max = std::max(smem_fit_max, sm);
   }
   P->n_d = od;
   P->n_i = oi;
   P->n_f = of;
   P->n_traj = ot;
-  // stage the factorization in shared memory when it fits the opt-in limit,
-  // otherwise keep its scratch in the solve's global work area
-  const size_t optin = size_t(ctx().smem_optin > 0 ? ctx().smem_optin : 232448);
-  P->fac_global = smem_max > optin ? 1 : 0;
-  // ADMM iterates of the IC projection in shared memory when they fit
-  size_t ic = 0;
-  for (auto& d : P->descs) ic = std::max(ic, fpe_ic_admm_bytes(d.cap_dof_s, d.cap_dof_v));
+  // Launch with the largest shared-memory need among the solves whose
+  // factorization scratch fits the opt-in limit; each solve that does not fit
+  // keeps its scratch in its global work area (decided per solve by the
+  // kernel), so one wide grid does not move a whole mixed batch to global.
+  P->fac_global = 0;
+  P->radau_smem = std::max(smem_fit_max, smem_base_max);
+  // ADMM iterates of the IC projection in shared memory, per solve, when they fit
   const size_t ic_lim = optin - sizeof(fpe::IcSmem) - 1024;
-  P->ic_smem = ic <= ic_lim ? ic : 0;
-  P->radau_smem = P->fac_global ? smem_base_max : smem_max;
+  size_t ic = 0;
+  for (auto& d : P->descs) {
+    const size_t need = fpe_ic_admm_bytes(d.cap_dof_s, d.cap_dof_v);
+    if (need <= ic_lim) ic = std::max(ic, need);
+  }
+  P->ic_smem = ic;
   P->setup_smem = sizeof(fpe::SetupSmem);
   return 0;
 }
@@ -316,12 +321,12 @@ static int plan_launch(FpePlan* P, cudaStream_t s, int from, int to) {
     if (P->o.precision == 0) {
       fpe::RadauKernelArgs<double> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena,
                                      P->d_traj, 0, P->o.complex_mode, P->fac_global,
-                                     rk.u1, rk.alph, rk.beta, rk.ti13};
+                                     rk.u1, rk.alph, rk.beta, rk.ti13, P->radau_smem};
       fpe::k_radau<double><<<grid, block, P->radau_smem, s>>>(a);
     } else {
       fpe::RadauKernelArgs<float> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena,
                                     P->d_traj, P->o.refine, P->o.complex_mode, P->fac_global,
-                                    rk.u1, rk.alph, rk.beta, rk.ti13};
+                                    rk.u1, rk.alph, rk.beta, rk.ti13, P->radau_smem};
       fpe::k_radau<float><<<grid, block, P->radau_smem, s>>>(a);
     }
     ++launches;
@@ -1198,11 +1203,11 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
   const fpe::RadauConstants rk = fpe::radau_constants(o.radau_exact != 0);
   if (o.precision == 0) {
     fpe::RadauKernelArgs<double> a{g_desc, g_d, g_i, g_info, g_f, nullptr, 0, o.complex_mode,
-                                   fac_global, rk.u1, rk.alph, rk.beta, rk.ti13};
+                                   fac_global, rk.u1, rk.alph, rk.beta, rk.ti13, radau_smem};
     fpe::k_radau<double><<<grid, block, radau_smem, s>>>(a);
   } else {
     fpe::RadauKernelArgs<float> a{g_desc, g_d, g_i, g_info, g_f, nullptr, o.refine, o.complex_mode,
-                                  fac_global, rk.u1, rk.alph, rk.beta, rk.ti13};
+                                  fac_global, rk.u1, rk.alph, rk.beta, rk.ti13, radau_smem};
     fpe::k_radau<float><<<grid, block, radau_smem, s>>>(a);
   }
   fpe::k_payoff<<<grid, block, 0, s>>>(g_desc, g_d, g_i, g_info, g_k, g_p);

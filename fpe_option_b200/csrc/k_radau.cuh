@@ -125,7 +125,7 @@ struct RadauKernelArgs {
   double* traj;
   int nref;          // extra FP64 refinement sweeps per stage solve
   int complex_mode;  // 0 GMRES(10) with E1 preconditioner, 1 complex block LU
-  int fac_global;    // factorization scratch in global memory (too large for shared)
+  int fac_global;    // 1: every solve keeps its factorization scratch in global memory
   // Eigenvalues of the Radau IIA A^-1 (gamma, alpha +- i beta) and TI13 of the
   // transformation.  The reference hard-codes U1 = 3.6378165692476072,
   // ALPH = 2.6753213032678365, BETA = 3.0493570545593676 and
@@ -134,6 +134,8 @@ struct RadauKernelArgs {
   // 0.54177053993587487119.  The host passes the reference values for
   // reference-parity runs and the exact ones otherwise.
   double u1, alph, beta, ti13;
+  size_t smem_bytes;  // dynamic shared memory of the launch: a solve whose scratch
+                      // does not fit in it keeps the scratch in global memory
 };
 
 // The reference's stage constants (radau.mojo:64-75) and the exact ones.
@@ -177,11 +179,14 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
   // shared memory: RadauSmem | fs (4 ns 7) | fv (5 nv 7) | factor scratch
   double* fs = reinterpret_cast<double*>(smem_raw + sizeof(RadauSmem));
   double* fv = fs + 4 * ns * 7;
-  // factor scratch, 16-byte aligned (complex FP64 elements)
-  void* sbig = A.fac_global
-                   ? reinterpret_cast<void*>(D + DL.fsc)
-                   : reinterpret_cast<void*>((reinterpret_cast<uintptr_t>(fv + 5 * nv * 7) + 15) &
-                                             ~uintptr_t(15));
+  // factor scratch, 16-byte aligned (complex FP64 elements), in shared memory
+  // when this solve's scratch fits in the launch's dynamic shared memory
+  const int esz = int(sizeof(FT));
+  const uintptr_t s_fac = (reinterpret_cast<uintptr_t>(fv + 5 * nv * 7) + 15) & ~uintptr_t(15);
+  const size_t fac_need = size_t(fpe_fac_scratch_elems(nv)) * esz * (direct ? 3 : 1) + (direct ? 16 : 0);
+  const bool fac_shared =
+      !A.fac_global && (s_fac - reinterpret_cast<uintptr_t>(smem_raw)) + fac_need <= A.smem_bytes;
+  void* sbig = fac_shared ? reinterpret_cast<void*>(s_fac) : reinterpret_cast<void*>(D + DL.fsc);
   for (int e = threadIdx.x; e < 4 * ns * 7; e += blockDim.x) fs[e] = D[DL.op_s + e];
   for (int e = threadIdx.x; e < 5 * nv * 7; e += blockDim.x) fv[e] = D[DL.op_v + e];
   if (threadIdx.x == 0) {
@@ -200,10 +205,7 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
   const BlockLU<Cx<FT>> LC{reinterpret_cast<Cx<FT>*>(fbase + size_t(ns) * 7 * bs), ns, nv, bs};
   // Staged sweeps when the stage buffers fit in the (shared) factorization
   // scratch, which is idle while the sweeps run.
-  const int esz = int(sizeof(FT));
-  const long long fac_bytes = A.fac_global ? 0
-                              : (long long)fpe_fac_scratch_elems(nv) * esz *
-                                        (direct ? 3 : 1) + (direct ? 16 : 0);
+  const long long fac_bytes = fac_shared ? (long long)fac_need : 0;
   const bool staged = fac_bytes >= stage_total_bytes(nv, esz, direct);
   SolveStage SP;
   SP.slot_r = stage_slot_bytes(nv, esz);
