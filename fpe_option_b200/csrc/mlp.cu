@@ -40,7 +40,7 @@ using bf16 = __nv_bfloat16;
 constexpr int kTileM = 128;
 constexpr int kTileN = 256;
 constexpr int kChunkK = 64;
-constexpr int kThreads = 128;
+constexpr int kThreads = 256;  // two warpgroups: both stage operands and split the epilogue's columns
 constexpr int kBufBytes = (kTileM + kTileN) * kChunkK * 2;  // one A + B chunk
 constexpr int kSmemBytes = 2 * kBufBytes;                    // double buffered (96 KB: <= 2 CTAs per SM)
 
@@ -144,14 +144,18 @@ struct GemmParams {
 
 // Stage rows [row0, row0 + rows) x K [k0, k0 + kc) of a K-contiguous BF16
 // matrix into the canonical layout: core matrix (row / 8, k / 8) at
-// ((row / 8) * (kc / 8) + k / 8) * 128 bytes, row % 8 at 16 bytes each.
+// ((row / 8) * (kc / 8) + k / 8) * 128 bytes, row % 8 at 16 bytes each.  Each
+// 16-byte piece moves by an asynchronous copy, so all of a thread's pieces are
+// in flight together (completed by cp_async_wait_all).  Consecutive threads
+// fill consecutive 16-byte rows of one core matrix (bank-conflict free).
 __device__ __forceinline__ void stage_kmajor(unsigned char* dst, const bf16* src, int ld, int row0, int rows,
                                              int k0, int kc) {
   const int k8n = kc >> 3;
   for (int v = threadIdx.x; v < rows * k8n; v += blockDim.x) {
-    const int r = v / k8n, j = v - r * k8n;
-    const uint4 val = *reinterpret_cast<const uint4*>(src + size_t(row0 + r) * ld + k0 + 8 * j);
-    *reinterpret_cast<uint4*>(dst + ((r >> 3) * k8n + j) * 128 + (r & 7) * 16) = val;
+    const int q = v >> 3, rr = v & 7;     // core matrix q = (row group, k group)
+    const int rg = q / k8n, j = q - rg * k8n;
+    const int r = rg * 8 + rr;
+    cp_async_elem<16>(dst + size_t(q) * 128 + rr * 16, src + size_t(row0 + r) * ld + k0 + 8 * j);
   }
 }
 
@@ -191,6 +195,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
     stage_kmajor(bufB[b], P.B, P.ldb, n0, Nt, k0, kc);
   };
   if (nchunk > 0) load(0, 0);
+  cp_async_wait_all();
   fence_proxy_async_smem();
   __syncthreads();
   for (int c = 0; c < nchunk; ++c) {
@@ -216,6 +221,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
       umma_commit(&bar[b]);
     }
     if (c + 1 < nchunk) load(c + 1, b ^ 1);
+    cp_async_wait_all();
     fence_proxy_async_smem();
     __syncthreads();
   }
@@ -230,10 +236,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
   }
   ok = __syncthreads_and(ok ? 1 : 0) != 0;
   if (ok && nchunk > 0) {
-    const int r = 32 * warp + lane;
+    // warp w reads TMEM lanes 32 (w % 4) .. + 31 (tile rows); the two
+    // warpgroups take alternate 16-column chunks of the accumulator
+    const int quarter = warp & 3, half = warp >> 2;
+    const int r = 32 * quarter + lane;
     const int gm = m0 + r;
-    const uint32_t trow = tmem + (uint32_t(32 * warp) << 16);
-    for (int c = 0; c < Nt; c += 16) {
+    const uint32_t trow = tmem + (uint32_t(32 * quarter) << 16);
+    for (int c = 16 * half; c < Nt; c += 32) {
       float v[16];
       tmem_ld16(trow + uint32_t(c), v);
       const int gn = n0 + c;
@@ -539,6 +548,11 @@ struct FpeMlp {
   bf16 *dZb[2] = {nullptr, nullptr}, *dZbT[2] = {nullptr, nullptr};
   float *yhat = nullptr, *dy = nullptr, *loss = nullptr;
   int* err = nullptr;
+  // inference: rows per launch sequence and its own buffers
+  int irows = 0;
+  bf16* Xi = nullptr;
+  bf16* Hi[2] = {nullptr, nullptr};
+  float* yi = nullptr;
   int* step = nullptr;          // Adam step counter (device)
   float* hyper = nullptr;       // {lr, 1 - b1^t, 1 - b2^t} of the current step (device)
   float* lr_table = nullptr;    // learning-rate schedule (device), lr_len entries
@@ -573,15 +587,15 @@ int mlp_cast_all(FpeMlp* M, cudaStream_t s) {
 }
 
 // Forward over rows [0, rows) of the packed input; keep = 1 stores Z and H^T
-// (training), otherwise only H (inference).
+// (training buffers), otherwise only H (inference buffers Xi, Hi, yi).
 int mlp_forward_packed(FpeMlp* M, int rows, bool keep, cudaStream_t s) {
   using namespace fpe::mlp;
-  const bf16* in = M->X;
+  const bf16* in = keep ? M->X : M->Xi;
   int ld_in = M->in_pad;
   for (int l = 0; l < M->layers; ++l) {
     GemmParams P = gp(in, ld_in, M->Wb[l], M->in_of(l), rows, M->hidden, M->in_of(l), EPI_BIAS_SILU, M->err);
     P.bias = M->theta + M->off_b[l];
-    P.Cb = keep ? M->H[l] : M->H[l & 1];
+    P.Cb = keep ? M->H[l] : M->Hi[l & 1];
     P.ldcb = M->hidden;
     if (keep) {
       P.Cf = M->Z[l];
@@ -593,9 +607,9 @@ int mlp_forward_packed(FpeMlp* M, int rows, bool keep, cudaStream_t s) {
     in = P.Cb;
     ld_in = M->hidden;
   }
-  const bf16* last = keep ? M->H[M->layers - 1] : M->H[(M->layers - 1) & 1];
+  const bf16* last = keep ? M->H[M->layers - 1] : M->Hi[(M->layers - 1) & 1];
   k_out_forward<<<(rows * 32 + 255) / 256, 256, 0, s>>>(last, M->hidden, rows, M->theta + M->off_wo,
-                                                         M->theta + M->off_bo, M->yhat);
+                                                         M->theta + M->off_bo, keep ? M->yhat : M->yi);
   MK(cudaGetLastError());
   return 0;
 }
@@ -719,6 +733,9 @@ FpeMlp* fpe_mlp_create(int32_t n_in, int32_t hidden, int32_t layers, int32_t max
   bad = bad || M->alloc(&M->X, R * M->in_pad) || M->alloc(&M->XT, R * M->in_pad) || M->alloc(&M->yhat, R) ||
         M->alloc(&M->dy, R) || M->alloc(&M->loss, 1) || M->alloc(&M->err, 1) || M->alloc(&M->step, 1) ||
         M->alloc(&M->hyper, 4);
+  M->irows = std::max(M->rows, 65536);
+  bad = bad || M->alloc(&M->Xi, size_t(M->irows) * M->in_pad) || M->alloc(&M->Hi[0], size_t(M->irows) * hidden) ||
+        M->alloc(&M->Hi[1], size_t(M->irows) * hidden) || M->alloc(&M->yi, size_t(M->irows));
   if (bad || cudaMemcpy(M->theta, h.data(), size_t(o) * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
       mlp_cast_all(M, mctx().stream) || cudaStreamSynchronize(mctx().stream) != cudaSuccess) {
     delete M;
@@ -767,13 +784,13 @@ int32_t fpe_mlp_set_params(FpeMlp* M, const float* in, int64_t n) {
 int32_t fpe_mlp_forward(FpeMlp* M, const float* x, int32_t n, float* y, void* stream) {
   if (!M || !x || !y || n < 0) return -1;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : mctx().stream;
-  for (int32_t r0 = 0; r0 < n; r0 += M->rows) {
-    const int cnt = std::min(M->rows, n - r0);
+  for (int32_t r0 = 0; r0 < n; r0 += M->irows) {
+    const int cnt = std::min(M->irows, n - r0);
     const int rows = (cnt + 127) & ~127;
     fpe::mlp::k_pack_input<<<grid_for(int64_t(rows) * M->in_pad), 256, 0, s>>>(
-        x + size_t(r0) * M->n_in, cnt, M->n_in, M->in_pad, rows, M->X, nullptr);
+        x + size_t(r0) * M->n_in, cnt, M->n_in, M->in_pad, rows, M->Xi, nullptr);
     if (mlp_forward_packed(M, rows, false, s)) return -1;
-    MK(cudaMemcpyAsync(y + r0, M->yhat, size_t(cnt) * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    MK(cudaMemcpyAsync(y + r0, M->yi, size_t(cnt) * sizeof(float), cudaMemcpyDeviceToDevice, s));
   }
   MK(cudaGetLastError());
   return 0;

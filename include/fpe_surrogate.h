@@ -24,8 +24,8 @@ typedef struct FpeMlp FpeMlp;
 /** Creates a network with n_in inputs (padded internally to a multiple of 16),
  *  `layers` hidden layers of width `hidden` (128 or 256: the weight-gradient
  *  products tile the hidden dimension by 128 tensor-memory lanes) and
- *  one output, able to process `max_rows` rows per call (training and
- *  inference; inference splits larger inputs).  Weights are initialised like
+ *  one output, training on up to `max_rows` rows per step; inference takes any
+ *  number of rows, in launch sequences of max(max_rows, 65536) rows.  Weights are initialised like
  *  a default linear layer, U(-1/sqrt(fan_in), 1/sqrt(fan_in)), from `seed`.
  *  Returns NULL on a bad argument or without a GPU. */
 extern FpeMlp* fpe_mlp_create(int32_t n_in, int32_t hidden, int32_t layers, int32_t max_rows,
