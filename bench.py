@@ -118,6 +118,27 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+def rank_seed(seed: int, rank: int) -> int:
+    """Each rank prices its own batch: weak scaling, no data-path collective."""
+    return seed + rank
+
+
+def max_over_ranks(x: float, dist, world: int, device) -> float:
+    """The slowest rank's time (every rank takes the same collective step)."""
+    if world <= 1:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world: int, per_rank: int, steps: int, seconds: float) -> float:
+    """Whole-job rate: the units all ranks processed over the slowest rank's time."""
+    return world * per_rank * steps / seconds
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -224,7 +245,7 @@ def main():
     if not fpe.is_available():
         raise RuntimeError("CUDA engine unavailable")
     nc = args.contracts
-    P, I = make_batch(nc, args.seed + rank)
+    P, I = make_batch(nc, rank_seed(args.seed, rank))
     opts = fpe.BatchOptions(disc=1, precision=args.precision, rtol=args.rtol,
                             atol=args.rtol * 1e-2, complex_solve=2, radau_constants=2)
     arr, keep = fpe.contracts_from_arrays(P, I)
@@ -262,13 +283,10 @@ def main():
             plan.run(sptr)
         e1.record(stream)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, world, "cuda")
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * nc * args.steps / (ms / 1000.0)
+    value = aggregate_rate(world, nc, args.steps, ms / 1000.0)
     # ---- end to end through the public C ABI (host contracts -> host prices) -----
     pinned = torch.empty((nc, 12), dtype=torch.float64).pin_memory()
     pinned.copy_(torch.from_numpy(P))
@@ -286,12 +304,8 @@ def main():
         pe, _, _, _, _ = pl.results()
         pl.close()
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * nc * args.steps / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, world, "cuda")
+    e2e = aggregate_rate(world, nc, args.steps, e2e_s)
     # ---- roofline of k_radau -----------------------------------------------------
     peak, peak_kind = load_peaks()
     radau_ms = ktimes[3]
