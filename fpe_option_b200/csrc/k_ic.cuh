@@ -360,7 +360,8 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_ic(const FpeSolveDesc* __restr
   __syncthreads();
   jacobi_eig(nds, As, Vs, S.cs, S.red);
   jacobi_eig(ndv, Av, Vv, S.cs, S.red);
-  const double rho = 0.1, sigma = 1e-6, lamreg = 1e-6, eps_abs = 1e-8, eps_rel = 1e-8;
+  const double sigma = 1e-6, lamreg = 1e-6, eps_abs = 1e-8, eps_rel = 1e-8;
+  double rho = 0.1;
   const double alpha = lamreg + sigma + rho;
   for (int e = threadIdx.x; e < N; e += blockDim.x) {
     const int a = e / ndv, b = e - a * ndv;
@@ -470,6 +471,28 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_ic(const FpeSolveDesc* __restr
     if (sqrt(nr[0]) < eps_p && sqrt(nr[1]) < eps_d) {
       ++it;
       break;
+    }
+    // Config discretization: residual balancing of rho (Boyd et al. 2011,
+    // sec. 3.4.1) every 10 iterations -- x2 when the primal residual exceeds
+    // 10x the dual one, /2 in the opposite case; the scaled dual u is rescaled
+    // and the diagonal of the fast diagonalization recomputed.  The reference
+    // discretization keeps the reference's fixed rho.
+    if (d.disc == 1 && (it + 1) % 10 == 0) {
+      const double rp = sqrt(nr[0]), rd = sqrt(nr[1]);
+      double f = 1.0;
+      if (rp > 10.0 * rd && rho < 1e6) f = 2.0;
+      else if (rd > 10.0 * rp && rho > 1e-6) f = 0.5;
+      if (f != 1.0) {
+        rho *= f;
+        const double al = lamreg + sigma + rho;
+        for (int e = threadIdx.x; e < N; e += blockDim.x) {
+          const int a = e / ndv, b = e - a * ndv;
+          const double ls = As[a * nds + a], lv = Av[b * ndv + b];
+          slam[e] = 1.0 / ((ls * ls) * (lv * lv) + al);
+          su[e] /= f;
+        }
+        __syncthreads();
+      }
     }
   }
   if (sz != z) {

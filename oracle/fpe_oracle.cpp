@@ -837,9 +837,14 @@ static int csr_kl(const CSR& A) {
   return k;
 }
 
-static Vec nnls_admm(const CSR& M, const Vec& b, long* iters) {  // osqp.mojo:52-159
+// adaptive: residual balancing of rho (Boyd et al. 2011, sec. 3.4.1) every 10
+// iterations -- rho x2 when the primal residual exceeds 10x the dual one, /2
+// in the opposite case, the scaled dual rescaled accordingly.  Off for the
+// reference discretization (its fixed rho = 0.1), on for the config one.
+static Vec nnls_admm(const CSR& M, const Vec& b, long* iters, bool adaptive = false) {  // osqp.mojo:52-159
   const int max_iter = 50000;
-  const double eps_abs = 1e-8, eps_rel = 1e-8, rho = 0.1, sigma = 1e-6, lam = 1e-6;
+  const double eps_abs = 1e-8, eps_rel = 1e-8, sigma = 1e-6, lam = 1e-6;
+  double rho = 0.1;
   int n = M.ncols;
   if (n == 0) return {};
   CSR Mt = csr_transpose(M);
@@ -883,6 +888,26 @@ static Vec nnls_admm(const CSR& M, const Vec& b, long* iters) {  // osqp.mojo:52
     if (std::sqrt(pr) < eps_p && std::sqrt(du) < eps_d) {
       ++it;
       break;
+    }
+    if (adaptive && (it + 1) % 10 == 0) {
+      const double rp = std::sqrt(pr), rd = std::sqrt(du);
+      double f = 1.0;
+      if (rp > 10.0 * rd && rho < 1e6) f = 2.0;
+      else if (rd > 10.0 * rp && rho > 1e-6) f = 0.5;
+      if (f != 1.0) {
+        const double old_alpha = lam + sigma + rho;
+        rho *= f;
+        const double new_alpha = lam + sigma + rho;
+        for (int i = 0; i < n; ++i) {
+          u[i] /= f;
+          for (int p = MtM.indptr[i]; p < MtM.indptr[i + 1]; ++p)
+            if (MtM.indices[p] == i) {
+              MtM.data[p] += new_alpha - old_alpha;
+              break;
+            }
+        }
+        lu.factor(MtM);
+      }
     }
   }
   if (iters) *iters = it;
@@ -1534,7 +1559,7 @@ struct Pipeline {
     Vec bsc(N);
     for (int i = 0; i < N; ++i) bsc[i] = Dinv[i] * proj[i];
     Vec c = opt.nnls_exact ? nnls_exact(gs, bsc, &admm_iters)
-                                              : nnls_admm(gs, bsc, &admm_iters);
+                                              : nnls_admm(gs, bsc, &admm_iters, opt.disc == 1);
     q0.assign(N, 0.0);
     for (int i = 0; i < N; ++i) {
       q0[i] = Dinv[i] * c[i];

@@ -256,15 +256,16 @@ def test_config0_single_contract(engine, oracle):
     r 0.1, kappa 1.2, theta 0.05, eta 0.35, rho -0.4, T 0.6, call K 60 on
     [0, 180] x [0, 1], 40 x 24 sinh knots, 4-point Gauss-Legendre per span,
     IC sigma (0.6, 0.004), rtol 1e-8, atol 1e-10.  The device solve matches the
-    oracle's on the same discretization to 1e-9 (FP64) and 1e-6 (mixed); the
-    characteristic-function price states the discretization error (reported,
-    loose bound)."""
+    oracle's on the same discretization to 1e-7 (FP64: both sides solve the IC
+    projection to the ADMM tolerance 1e-8, with different linear algebra) and
+    1e-6 (mixed); the characteristic-function price states the discretization
+    error (reported, loose bound)."""
     fpe = engine
     P = np.array([[1.2, 0.05, 0.35, -0.4, 0.1, 0.6, 60.0, 0.1, 60.0, 0.0, 0.0, 180.0]])
     I = np.array([[40, 24, 8]], np.int32)
     ref = oracle.price_batch(P, I, oracle.options(disc=1, rtol=1e-8, atol=1e-10, complex_direct=1,
                                                   radau_constants=2))
-    for prec, tol in ((0, 1e-9), (1, 1e-6)):
+    for prec, tol in ((0, 1e-7), (1, 1e-6)):
         got, st = fpe.price_batch(P, I, fpe.BatchOptions(disc=1, precision=prec, rtol=1e-8, atol=1e-10,
                                                          complex_solve=2, radau_constants=2))
         assert st[0] == 0
