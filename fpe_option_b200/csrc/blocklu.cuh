@@ -428,18 +428,27 @@ __device__ bool fac_gj_warp(FacScratch<ET>& S) {
       S.pinv[c] = inv;
     }
     __syncwarp();  // every lane has read a_pc before the owner overwrites it
-    if (own0 && r0 != p) {
-      const ET f = fmul(a0[c], inv);
-#pragma unroll 4
-      for (int l = 0; l < nv; ++l) a0[l] = fsub(a0[l], fmul(f, ap[l]));
-      a0[c] = fsub(fzero(ET()), f);
-    }
-    if (own1 && r1 != p) {
-      const ET f = fmul(a1[c], inv);
-#pragma unroll 4
-      for (int l = 0; l < nv; ++l) a1[l] = fsub(a1[l], fmul(f, ap[l]));
-      a1[c] = fsub(fzero(ET()), f);
-    }
+    // row -= f * pivot row, in 8-element chunks loaded to registers before any
+    // store (the rows never alias, but the compiler cannot know), so the
+    // shared-memory loads of a chunk overlap instead of forming one chain
+    auto eliminate = [&](ET* row) {
+      const ET f = fmul(row[c], inv);
+      int l = 0;
+      for (; l + 8 <= nv; l += 8) {
+        ET pv[8], rv[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          pv[k] = ap[l + k];
+          rv[k] = row[l + k];
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) row[l + k] = fsub(rv[k], fmul(f, pv[k]));
+      }
+      for (; l < nv; ++l) row[l] = fsub(row[l], fmul(f, ap[l]));
+      row[c] = fsub(fzero(ET()), f);
+    };
+    if (own0 && r0 != p) eliminate(a0);
+    if (own1 && r1 != p) eliminate(a1);
     if (p == r0) a0[c] = fone(ET());
     if (p == r1) a1[c] = fone(ET());
     __syncwarp();
@@ -736,7 +745,8 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
 // --------------------------------------------------------------------------
 struct SolveStage {
   unsigned char* buf[2];     // stage buffers (shared, 16-byte aligned)
-  double* ring;              // 4 segments x nv per right-hand-side array (nr real, re, im)
+  void* ring;                // 4 segments x nv per right-hand-side array (nr real, re, im), of the
+                             // sweep's accumulation type (float with FP32 factors, else double)
   unsigned long long* bar;   // 2 mbarriers (shared)
   int* err;                  // shared flag: a bounded wait gave up
   int slot_r, slot_c;        // bytes per staged real / complex block slot
@@ -796,7 +806,47 @@ __device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s) {
   }
 }
 
-// a += sum_m col[m nv] x[m] with two accumulators (col: shared, transposed block)
+// a += sum_m col[m nv] x[m] with independent accumulators (col: shared,
+// transposed block).  With FP32 factors the sweep accumulates in FP32: the
+// factor's own rounding is of the same order, and the FP64 Newton residual
+// corrects whatever the preconditioner apply leaves.
+__device__ __forceinline__ void col_dot(const float* col, const float* x, int nv, float& a) {
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+  int m = 0;
+  for (; m + 3 < nv; m += 4) {
+    a0 = fmaf(col[m * nv], x[m], a0);
+    a1 = fmaf(col[(m + 1) * nv], x[m + 1], a1);
+    a2 = fmaf(col[(m + 2) * nv], x[m + 2], a2);
+    a3 = fmaf(col[(m + 3) * nv], x[m + 3], a3);
+  }
+  for (; m < nv; ++m) a0 = fmaf(col[m * nv], x[m], a0);
+  a += (a0 + a1) + (a2 + a3);
+}
+__device__ __forceinline__ void col_dot_c(const Cx<float>* col, const float* xr, const float* xi, int nv, float& ar,
+                                          float& ai) {
+  float r0 = 0.f, r1 = 0.f, i0 = 0.f, i1 = 0.f;
+  int m = 0;
+  for (; m + 1 < nv; m += 2) {
+    const Cx<float> b0 = col[m * nv], b1 = col[(m + 1) * nv];
+    r0 = fmaf(b0.re, xr[m], r0);
+    r0 = fmaf(-b0.im, xi[m], r0);
+    i0 = fmaf(b0.re, xi[m], i0);
+    i0 = fmaf(b0.im, xr[m], i0);
+    r1 = fmaf(b1.re, xr[m + 1], r1);
+    r1 = fmaf(-b1.im, xi[m + 1], r1);
+    i1 = fmaf(b1.re, xi[m + 1], i1);
+    i1 = fmaf(b1.im, xr[m + 1], i1);
+  }
+  if (m < nv) {
+    const Cx<float> b0 = col[m * nv];
+    r0 = fmaf(b0.re, xr[m], r0);
+    r0 = fmaf(-b0.im, xi[m], r0);
+    i0 = fmaf(b0.re, xi[m], i0);
+    i0 = fmaf(b0.im, xr[m], i0);
+  }
+  ar += r0 + r1;
+  ai += i0 + i1;
+}
 __device__ __forceinline__ void col_dot(const float* col, const double* x, int nv, double& a) {
   double a0 = 0.0, a1 = 0.0;
   int m = 0;
@@ -819,7 +869,7 @@ __device__ __forceinline__ void col_dot(const double* col, const double* x, int 
 }
 template <typename T>
 __device__ __forceinline__ void col_dot_c(const Cx<T>* col, const double* xr, const double* xi, int nv, double& ar,
-                                          double& ai) {
+                                          double& ai) {  // FP64 accumulation
   double r0 = 0.0, i0 = 0.0;
   for (int m = 0; m < nv; ++m) {
     const Cx<T> b = col[m * nv];
@@ -854,9 +904,11 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
   const bool is_c = S.nc > 0 && tid >= cbase && tid < cbase + Gc * nv;
   const int cu = is_c ? tid - cbase : 0;
   const int cj = cu / Gc, cg = cu - cj * Gc;
+  using RT = FT;  // accumulation / ring type: float with FP32 factors, double with FP64
   const int nv4 = 4 * nv;
-  double* ring_c_re = P.ring + S.nr * nv4;
-  double* ring_c_im = ring_c_re + nv4;
+  RT* ringb = static_cast<RT*>(P.ring);
+  RT* ring_c_re = ringb + S.nr * nv4;
+  RT* ring_c_im = ring_c_re + nv4;
 
   uint32_t pend = 0;  // buffers with a stage in flight (thread 0's view)
   if (tid == 0) {
@@ -883,25 +935,25 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
     const int i = fwd ? s : 2 * ns - s;
     if (ok) {
       if (is_r) {
-        const double* ring = P.ring + rsys * nv4;
-        double a = 0.0, z = 0.0;
+        const RT* ring = ringb + rsys * nv4;
+        RT a = RT(0), z = RT(0);
         if (fwd) {
           for (int g = 0; g < 3; ++g)
             if (i < ns && i - 3 + g >= 0)
               col_dot(reinterpret_cast<const FT*>(buf + g * P.slot_r) + rj, ring + ((i - 3 + g) & 3) * nv, nv, a);
           if (i >= 1) col_dot(reinterpret_cast<const FT*>(buf + 3 * P.slot_r) + rj, ring + ((i - 1) & 3) * nv, nv, z);
-          if (i < ns) P.ring[rsys * nv4 + (i & 3) * nv + rj] = S.xr[rsys][i * nv + rj] - a;
-          if (i >= 1) S.zr[rsys][(i - 1) * nv + rj] = z;
+          if (i < ns) ringb[rsys * nv4 + (i & 3) * nv + rj] = RT(S.xr[rsys][i * nv + rj] - double(a));
+          if (i >= 1) S.zr[rsys][(i - 1) * nv + rj] = double(z);
         } else {
           for (int g = 0; g < 3; ++g)
             if (i + 1 + g < ns)
               col_dot(reinterpret_cast<const FT*>(buf + g * P.slot_r) + rj, ring + ((i + 1 + g) & 3) * nv, nv, a);
-          const double x = S.zr[rsys][i * nv + rj] - a;
-          P.ring[rsys * nv4 + (i & 3) * nv + rj] = x;
+          const double x = S.zr[rsys][i * nv + rj] - double(a);
+          ringb[rsys * nv4 + (i & 3) * nv + rj] = RT(x);
           S.xr[rsys][i * nv + rj] = x;
         }
       }
-      double ar = 0.0, ai = 0.0, zr = 0.0, zi = 0.0;
+      RT ar = RT(0), ai = RT(0), zr = RT(0), zi = RT(0);
       if (is_c) {
         const unsigned char* cb = buf + 4 * P.slot_r;
         for (int g = cg; g < 4; g += Gc) {
@@ -932,17 +984,17 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
       if (is_c && cg == 0) {
         if (fwd) {
           if (i < ns) {
-            ring_c_re[(i & 3) * nv + cj] = S.xc_re[i * nv + cj] - ar;
-            ring_c_im[(i & 3) * nv + cj] = S.xc_im[i * nv + cj] - ai;
+            ring_c_re[(i & 3) * nv + cj] = RT(S.xc_re[i * nv + cj] - double(ar));
+            ring_c_im[(i & 3) * nv + cj] = RT(S.xc_im[i * nv + cj] - double(ai));
           }
           if (i >= 1) {
-            S.zc_re[(i - 1) * nv + cj] = zr;
-            S.zc_im[(i - 1) * nv + cj] = zi;
+            S.zc_re[(i - 1) * nv + cj] = double(zr);
+            S.zc_im[(i - 1) * nv + cj] = double(zi);
           }
         } else {
-          const double xr = S.zc_re[i * nv + cj] - ar, xi = S.zc_im[i * nv + cj] - ai;
-          ring_c_re[(i & 3) * nv + cj] = xr;
-          ring_c_im[(i & 3) * nv + cj] = xi;
+          const double xr = S.zc_re[i * nv + cj] - double(ar), xi = S.zc_im[i * nv + cj] - double(ai);
+          ring_c_re[(i & 3) * nv + cj] = RT(xr);
+          ring_c_im[(i & 3) * nv + cj] = RT(xi);
           S.xc_re[i * nv + cj] = xr;
           S.xc_im[i * nv + cj] = xi;
         }

@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
   SP.slot_c = stage_slot_bytes(nv, 2 * esz);
   SP.buf[0] = reinterpret_cast<unsigned char*>(sbig);
   SP.buf[1] = SP.buf[0] + 4 * SP.slot_r + (direct ? 4 * SP.slot_c : 0);
-  SP.ring = reinterpret_cast<double*>(SP.buf[1] + 4 * SP.slot_r + (direct ? 4 * SP.slot_c : 0));
+  SP.ring = reinterpret_cast<void*>(SP.buf[1] + 4 * SP.slot_r + (direct ? 4 * SP.slot_c : 0));
   SP.bar = S.pipe_bar;
   SP.err = &S.pipe_err;
   uint32_t pipe_phase = 0;
