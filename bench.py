@@ -202,6 +202,8 @@ def main():
     ap.add_argument("--precision", type=int, default=1)
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-surrogate-rate", dest="surrogate_rate", action="store_false",
+                    help="skip the surrogate inference rate in the batch line")
     ap.add_argument("--plain-sample", type=int, default=8,
                     help="contracts timed on the plain one-solve-per-launch FP64 path")
     ap.add_argument("--workload", default="batch", choices=["batch", "barrier", "surrogate", "calibration"],
@@ -320,6 +322,28 @@ def main():
         cpu = {"value": rate, "unit": "prices/s", "cores": cores, "kind": "port",
                "sample": f"first {sample} contracts of the same batch, oracle C++ FP64 "
                          f"restatement on {cores} host threads, {dt:.1f} s"}
+    # ---- surrogate inference rate (3-member BF16 tensor-core ensemble) ---------------
+    sur = None
+    if rank == 0 and world == 1 and args.surrogate_rate:
+        from fpe_option_b200.surrogate import SurrogateConfig, SurrogatePricer, draw_contracts, encode
+
+        pr = SurrogatePricer(SurrogateConfig(members=3))
+        Q, J = draw_contracts(1 << 20, seed=7, kind="mixed", grid=(48, 24))
+        xq = torch.as_tensor(encode(Q, J)[0], device="cuda")
+        for _ in range(3):
+            pr.predict_features(xq)
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(5):
+            pr.predict_features(xq)
+        s1.record()
+        torch.cuda.synchronize()
+        sms = s0.elapsed_time(s1) / 5
+        sur = {"value": (1 << 20) / (sms / 1000.0), "unit": "prices/s", "queries": 1 << 20,
+               "note": "inference of the 3-member ensemble (untrained weights: the rate does not depend on "
+                       "them); trained accuracy: bench.py --workload surrogate / calibration"}
+        pr.close()
     # ---- plain path: one contract per launch sequence, FP64 factors ---------------
     plain = None
     if rank == 0 and world == 1 and args.plain_sample > 0:
@@ -366,6 +390,7 @@ def main():
                          "algorithmic_bytes": int(stats["factor_bytes"])},
             "cpu_baseline": cpu,
             "plain_fp64_one_per_launch": plain,
+            "surrogate_inference": sur,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

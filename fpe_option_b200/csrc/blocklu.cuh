@@ -119,24 +119,33 @@ struct BlockLU {
 template <typename ET>
 __device__ void blu_assemble(const OpFactors& O, const BlockLU<ET>& L, double a_re, double a_im,
                              double h) {
-  const int ns = O.ns, nv = O.nv, bs = L.bs;
-  const size_t total = size_t(ns) * 7 * bs;
-  for (size_t e = threadIdx.x; e < total; e += blockDim.x) {
-    const int jl = int(e % bs);
-    const int ikk = int(e / bs);
-    const int i = ikk / 7, kk = ikk - i * 7;
-    const int j = jl / nv, l = jl - j * nv;  // j >= nv: block padding
-    const int k = i + kk - 3, dl = l - j + 3;
-    double m = 0.0, kv = 0.0;
-    if (j < nv && k >= 0 && k < ns && dl >= 0 && dl < 7) {
-      const int sb = i * 7 + kk, vb = j * 7 + dl;
-      m = O.As[sb] * O.Av[vb];
-      kv = O.Ss[sb] * O.B1[vb] + O.Ts[sb] * O.B2[vb] + O.As[sb] * O.B3[vb] + O.St[sb] * O.B4[vb];
-    }
-    if constexpr (!IsCx<ET>::v) {
-      st_elem(L.F[e], a_re * m + h * kv);
-    } else {
-      st_elem(L.F[e], cmk(a_re * m + h * kv, a_im * m));
+  // Block by block: the blocks of a block row whose column lies outside the
+  // matrix (k < 0 or k >= ns) are never read, by the factorization or by the
+  // sweeps, and are not written; the padding after a block's nv^2 entries is
+  // not read either.  Row and column of entry e come from the exact float
+  // reciprocal (e < 2^16), not from integer divisions.
+  const int ns = O.ns, nv = O.nv, bs = L.bs, nn = nv * nv;
+  const float rnv = 1.0f / float(nv);
+  for (int blk = 0; blk < ns * 7; ++blk) {
+    const int i = blk / 7, kk = blk - 7 * i;
+    const int k = i + kk - 3;
+    if (k < 0 || k >= ns) continue;
+    const double as = O.As[blk], ss = O.Ss[blk], ts = O.Ts[blk], st = O.St[blk];
+    ET* B = L.F + size_t(blk) * bs;
+    for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+      const int j = int((float(e) + 0.5f) * rnv), l = e - j * nv;
+      const int dl = l - j + 3;
+      double m = 0.0, kv = 0.0;
+      if (dl >= 0 && dl < 7) {
+        const int vb = j * 7 + dl;
+        m = as * O.Av[vb];
+        kv = ss * O.B1[vb] + ts * O.B2[vb] + as * O.B3[vb] + st * O.B4[vb];
+      }
+      if constexpr (!IsCx<ET>::v) {
+        st_elem(B[e], a_re * m + h * kv);
+      } else {
+        st_elem(B[e], cmk(a_re * m + h * kv, a_im * m));
+      }
     }
   }
   __syncthreads();
