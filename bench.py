@@ -181,7 +181,7 @@ def run_reference_arm(args):
             "config": {"workload": f"{args.contracts} European Heston contracts, mixed grids 32-64 x 16-32",
                        "rtol": args.rtol, "contracts_per_step": sample},
             "cpu_baseline": {"value": v, "unit": "prices/s", "cores": cores, "kind": "port",
-                             "sample": f"{sample} contracts of the config-1 batch per step, "
+                             "sample": f"{sample} contracts of the bench batch per step, "
                                        f"oracle C++ FP64 restatement, {cores} threads"},
             "e2e": {"value": v, "unit": "prices/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -204,6 +204,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surrogate-rate", dest="surrogate_rate", action="store_false",
                     help="skip the surrogate inference rate in the batch line")
+    ap.add_argument("--no-cf-check", dest="cf_check", action="store_false",
+                    help="skip the characteristic-function check and rate in the batch line")
     ap.add_argument("--plain-sample", type=int, default=8,
                     help="contracts timed on the plain one-solve-per-launch FP64 path")
     ap.add_argument("--workload", default="batch", choices=["batch", "barrier", "surrogate", "calibration"],
@@ -344,6 +346,47 @@ def main():
                "note": "inference of the 3-member ensemble (untrained weights: the rate does not depend on "
                        "them); trained accuracy: bench.py --workload surrogate / calibration"}
         pr.close()
+    # ---- closed form: Heston characteristic-function prices of the same Europeans -----
+    cfb = None
+    if rank == 0 and world == 1 and args.cf_check:
+        from fpe_option_b200 import _lib
+
+        cf, cst = fpe.heston_cf_price(P, I)
+        ok = cst == 0
+        dev = np.abs(p_ref - cf)[ok] / np.maximum(np.abs(cf[ok]), 1e-3 * 100.0)
+        # the closed-form kernel's own rate on 2^18 device-resident prices
+        nq = 1 << 18
+        rep = np.resize(np.arange(nc), nq)
+        qP = torch.as_tensor(np.ascontiguousarray(P[rep][:, :8]), device="cuda")
+        qK = torch.as_tensor(np.ascontiguousarray(P[rep][:, 8]), device="cuda")
+        qput = torch.as_tensor((I[rep, 2] == 9).astype(np.int32), device="cuda")
+        qout = torch.empty(nq, dtype=torch.float64, device="cuda")
+        L = _lib.load()
+        for _ in range(3):
+            L.fpe_heston_cf_batch(qP.data_ptr(), qK.data_ptr(), qput.data_ptr(), nq, qout.data_ptr(), sptr)
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(3):
+            L.fpe_heston_cf_batch(qP.data_ptr(), qK.data_ptr(), qput.data_ptr(), nq, qout.data_ptr(), sptr)
+        c1.record(stream)
+        torch.cuda.synchronize()
+        cms = c0.elapsed_time(c1) / 3
+        # the error grows as the Feller ratio 2 kappa theta / sigma^2 falls: the variance
+        # density becomes singular at v = 0 and the v grid cannot follow it
+        feller = (2.0 * P[:, 0] * P[:, 1] / P[:, 2] ** 2)[ok]
+        bins = {}
+        for name, lo, hi in (("feller>=1", 1.0, np.inf), ("0.5<=feller<1", 0.5, 1.0),
+                             ("feller<0.5", 0.0, 0.5)):
+            m = (feller >= lo) & (feller < hi)
+            if m.any():
+                bins[name] = {"contracts": int(m.sum()), "median_rel_dev": float(np.median(dev[m])),
+                              "max_rel_dev": float(dev[m].max())}
+        cfb = {"fpe_vs_cf_median_rel_dev": float(np.median(dev)), "fpe_vs_cf_max_rel_dev": float(dev.max()),
+               "contracts": int(ok.sum()), "by_feller_ratio": bins, "cf_rate": nq / (cms / 1000.0),
+               "unit": "prices/s",
+               "note": "discretization error of the FPE prices (the tight-tolerance FP64 run of the same "
+                       "batch; floor 1e-3 S0) against the FP64 characteristic-function price; cf_rate: "
+                       "k_heston_cf on 2^18 device-resident prices"}
     # ---- plain path: one contract per launch sequence, FP64 factors ---------------
     plain = None
     if rank == 0 and world == 1 and args.plain_sample > 0:
@@ -391,6 +434,7 @@ def main():
             "cpu_baseline": cpu,
             "plain_fp64_one_per_launch": plain,
             "surrogate_inference": sur,
+            "closed_form_check": cfb,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -7,7 +7,8 @@ dataclasses and ``FpeParams``.  Everything computes on the GPU through the C
 ABI of ``libfpe_engine.so``; there is no CPU fallback.
 
 Additions: ``price_batch`` / ``Plan`` price thousands of contracts with
-different parameters, barriers and grid sizes in one launch sequence.
+different parameters, barriers and grid sizes in one launch sequence;
+``heston_cf_price`` prices Europeans from the Heston characteristic function.
 
 Usage::
 
@@ -33,7 +34,7 @@ _logger = logging.getLogger("fpe_engine")
 __all__ = [
     "price", "Compute", "FpeParams", "PriceResult", "KnotsResult", "GridPointsResult",
     "Basis1DResult", "GreeksResult", "is_available", "price_batch", "Plan", "Contract",
-    "BatchOptions", "OPTION_TYPES",
+    "BatchOptions", "OPTION_TYPES", "heston_cf_price",
 ]
 
 # python/fpe_engine/__init__.py:54-60
@@ -552,3 +553,27 @@ def price_batch(params: np.ndarray, ints: np.ndarray, options: BatchOptions | No
         finally:
             plan.close()
     return out_p, out_s
+
+
+def heston_cf_price(params: np.ndarray, ints: np.ndarray):
+    """European prices from the Heston characteristic function, FP64 on the GPU.
+
+    Same tables as :func:`price_batch` (grid columns are ignored); rows whose
+    option type is not 8 (call) or 9 (put) get NaN and status
+    ``FPE_STATUS_UNSUPPORTED`` (2).  Returns (prices, status).  No reference
+    counterpart: it measures the discretization error of the FPE prices."""
+    _require()
+    params = np.asarray(params)
+    ints = np.asarray(ints)
+    n = len(params)
+    prices = np.zeros(n)
+    status = np.zeros(n, np.int32)
+    if n == 0:
+        return prices, status
+    arr, keep = contracts_from_arrays(params, ints)
+    rc = _lib.load().fpe_heston_cf_price(arr, n, prices.ctypes.data_as(_lib.dp),
+                                         status.ctypes.data_as(_lib.ip))
+    del keep
+    if rc < 0:
+        raise RuntimeError("fpe_heston_cf_price failed")
+    return prices, status

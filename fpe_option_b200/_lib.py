@@ -66,7 +66,7 @@ EXPORTED = [
     "fpe_compute_free_oneshot", "fpe_plan_create", "fpe_plan_run", "fpe_plan_results",
     "fpe_plan_stats", "fpe_plan_sizes", "fpe_plan_destroy", "fpe_price_batch",
     "fpe_compute_create_ex", "fpe_compute_basis_csr", "fpe_device_available",
-    "fpe_plan_kernel_times", "fpe_price_noalloc",
+    "fpe_plan_kernel_times", "fpe_price_noalloc", "fpe_heston_cf_batch", "fpe_heston_cf_price",
     # include/fpe_surrogate.h
     "fpe_mlp_create", "fpe_mlp_destroy", "fpe_mlp_layout", "fpe_mlp_get_params",
     "fpe_mlp_set_params", "fpe_mlp_forward", "fpe_mlp_train_step", "fpe_mlp_gradient",
@@ -150,5 +150,9 @@ def load():
     L.fpe_gemm_bf16.argtypes = [vp, i32, vp, i32, i32, i32, i32, vp, i32, vp, i32, vp]
     L.fpe_price_noalloc.restype = i32
     L.fpe_price_noalloc.argtypes = [C.POINTER(FpeContract), C.POINTER(FpeBatchOptions), dp, ip, vp]
+    L.fpe_heston_cf_batch.restype = i32
+    L.fpe_heston_cf_batch.argtypes = [vp, vp, vp, i32, vp, vp]
+    L.fpe_heston_cf_price.restype = i32
+    L.fpe_heston_cf_price.argtypes = [C.POINTER(FpeContract), i32, dp, ip]
     _lib = L
     return L

@@ -28,8 +28,10 @@ quote falls back to the solver, whatever the members' disagreement, which is
 reported) and whose Jacobians are the surrogate's.  Its fixed point
 J_sur^T r_FPE = 0 is the FPE least-squares fit up to a term of second order
 in the Jacobian error times the residual, and each iteration costs one FPE
-pricing of the surface instead of eleven.  ``polish="fpe"`` uses FPE
-Jacobians instead; ``polish="none"`` keeps the surrogate's fit if its FPE
+pricing of the surface instead of eleven.  When no hybrid step lowers the
+FPE residual (the surrogate's Jacobian is no descent direction there, e.g.
+at a fit pinned to the edge of its training box), FPE Jacobians finish the
+polish.  ``polish="fpe"`` uses FPE Jacobians throughout; ``polish="none"`` keeps the surrogate's fit if its FPE
 residual RMS is within ``noise_ratio`` times the quotes' noise level.
 """
 from __future__ import annotations
@@ -60,6 +62,7 @@ class LMResult:
     residual_evals: int
     cost: float
     history: list = field(default_factory=list)
+    stop: str = "max_iter"  # gradient, xtol, ftol, max_rejects or max_iter
 
 
 def levenberg_marquardt(residual, jacobian, x0, max_iter: int = 50, tol: float = 1e-10,
@@ -81,6 +84,7 @@ def levenberg_marquardt(residual, jacobian, x0, max_iter: int = 50, tol: float =
     it = 0
     cost = np.inf
     rejects = 0
+    stop = "max_iter"
     for it in range(1, max_iter + 1):
         r, J = jacobian(x)
         evals += 1
@@ -88,6 +92,7 @@ def levenberg_marquardt(residual, jacobian, x0, max_iter: int = 50, tol: float =
         cost = float(r @ r)
         hist.append((cost, lam))
         if np.max(np.abs(g)) < tol:
+            stop = "gradient"
             break
         A = J.T @ J + lam * np.eye(len(x))
         delta = np.linalg.solve(A, -g)
@@ -100,16 +105,19 @@ def levenberg_marquardt(residual, jacobian, x0, max_iter: int = 50, tol: float =
             lam = max(lam * lambda_down, 1e-10)
             rejects = 0
             if xtol is not None and np.max(np.abs(delta)) <= xtol * (np.max(np.abs(x)) + xtol):
+                stop = "xtol"
                 break
             if ftol is not None and cost - c_new < ftol * cost:
                 cost = c_new
+                stop = "ftol"
                 break
         else:
             lam = lam * lambda_up
             rejects += 1
             if max_rejects is not None and rejects >= max_rejects:
+                stop = "max_rejects"
                 break
-    return LMResult(x=x, iterations=it, residual_evals=evals, cost=cost, history=hist)
+    return LMResult(x=x, iterations=it, residual_evals=evals, cost=cost, history=hist, stop=stop)
 
 
 @dataclass
@@ -305,14 +313,21 @@ def calibrate_with_surrogate(surface: Surface, pricer, x0, max_iter=50, tol=1e-1
     rms_fpe = float(np.sqrt(np.mean(r_fpe ** 2)))
     polished = False
     it_polish = 0
+    polish_used = polish
     if polish == "hybrid":
         hb = HybridSurface(fb, sb)
         # near-Gauss-Newton steps: the fit starts close to the optimum
         pol = levenberg_marquardt(hb.residual, hb.jacobian, x, max_iter=polish_iter, tol=tol,
                                   lambda_init=1e-9, **STOP)
+        it_polish = pol.iterations
+        if np.array_equal(pol.x, x) and pol.stop != "gradient":
+            # no step was accepted: the surrogate's Jacobian gives no descent
+            # direction for the FPE residual here, so the FPE's own finishes
+            polish_used = "hybrid->fpe"
+            pol = levenberg_marquardt(fb.residual, fb.jacobian, x, max_iter=polish_iter, tol=tol, **STOP)
+            it_polish += pol.iterations
         x = clamp(pol.x)
         polished = True
-        it_polish = pol.iterations
     elif polish == "fpe" or (polish == "none" and (quote_noise is None or rms_fpe > noise_ratio * quote_noise)):
         pol = levenberg_marquardt(fb.residual, fb.jacobian, x, max_iter=polish_iter, tol=tol, **STOP)
         x = clamp(pol.x)
@@ -320,7 +335,7 @@ def calibrate_with_surrogate(surface: Surface, pricer, x0, max_iter=50, tol=1e-1
         it_polish = pol.iterations
     return x, {"seconds": time.perf_counter() - t,
                "fpe_contracts": fb.contracts_priced + sb.contracts_priced,
-               "surrogate_iterations": res.iterations, "polished": polished,
+               "surrogate_iterations": res.iterations, "polished": polished, "polish": polish_used,
                "polish_iterations": it_polish, "fallback_quotes": sb.fallback_quotes,
                "max_disagreement_at_fit": spread, "x_surrogate_fit": x_sur.tolist(),
                "fpe_rms_at_surrogate_fit": rms_fpe,

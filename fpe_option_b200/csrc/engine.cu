@@ -20,6 +20,7 @@
 
 #include "../../include/fpe_engine.h"
 #include "fpe_device.h"
+#include "k_cf.cuh"
 #include "k_galerkin.cuh"
 #include "k_ic.cuh"
 #include "k_payoff.cuh"
@@ -1228,6 +1229,126 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
     prices[j] = v;
     if (status) status[j] = st;
     if (st && !worst) worst = st;
+  }
+  return worst;
+}
+
+// --------------------------------------------------------------------------
+// Heston characteristic-function prices of Europeans (k_cf.cuh)
+// --------------------------------------------------------------------------
+namespace {
+
+// 16-point Gauss-Legendre rule on [-1, 1]: Newton's method on the Legendre
+// polynomial P16 (three-term recurrence) from the Chebyshev-like guesses
+// cos(pi (i + 3/4) / (n + 1/2)); weights 2 / ((1 - x^2) P16'(x)^2).
+const fpe::CfNodes& cf_nodes() {
+  static fpe::CfNodes q;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    const int n = 16;
+    for (int i = 0; i < n; ++i) {
+      double z = std::cos(M_PI * (i + 0.75) / (n + 0.5)), dp = 1.0;
+      for (int it = 0; it < 100; ++it) {
+        double p = 1.0, pm = 0.0;
+        for (int k = 1; k <= n; ++k) {
+          const double pk = ((2.0 * k - 1.0) * z * p - (k - 1.0) * pm) / k;
+          pm = p;
+          p = pk;
+        }
+        dp = n * (z * p - pm) / (z * z - 1.0);
+        const double dz = p / dp;
+        z -= dz;
+        if (std::fabs(dz) < 1e-15) break;
+      }
+      q.x[i] = -z;
+      q.w[i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+  });
+  return q;
+}
+
+int launch_cf(const double* params, const double* strikes, const int32_t* put, int32_t n,
+              double* out, cudaStream_t s) {
+  const unsigned grid = unsigned((int64_t(n) + fpe::kCfWarps - 1) / fpe::kCfWarps);
+  fpe::k_heston_cf<<<grid, 32 * fpe::kCfWarps, 0, s>>>(params, strikes, put, n, cf_nodes(), out);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int32_t fpe_heston_cf_batch(const double* params_dev, const double* strikes_dev,
+                                       const int32_t* put_dev, int32_t n, double* prices_dev,
+                                       void* cuda_stream) {
+  if (n < 0) return -1;
+  if (n == 0) return 0;
+  if (!params_dev || !strikes_dev || !prices_dev) return -1;
+  Context& C = ctx();
+  if (!C.ok) return -1;
+  cudaStream_t s = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : C.stream;
+  return launch_cf(params_dev, strikes_dev, put_dev, n, prices_dev, s);
+}
+
+extern "C" int32_t fpe_heston_cf_price(const FpeContract* contracts, int32_t n, double* prices,
+                                       int32_t* status) {
+  if (n < 0 || (n > 0 && (!contracts || !prices))) return -1;
+  Context& C = ctx();
+  if (!C.ok) return -1;
+  // one row per strike: 8 parameters, the strike and the put flag, packed
+  // into one host buffer and copied with one transfer
+  int64_t m = 0;
+  for (int32_t c = 0; c < n; ++c) {
+    if (contracts[c].n_strikes < 0 || (contracts[c].n_strikes > 0 && !contracts[c].strikes)) return -1;
+    m += contracts[c].n_strikes;
+  }
+  if (m == 0) return 0;
+  if (m > INT32_MAX) return -1;
+  std::vector<int32_t> st(m, FPE_STATUS_OK);
+  const size_t pbytes = size_t(m) * 9 * sizeof(double), bytes = pbytes + size_t(m) * sizeof(int32_t);
+  std::vector<unsigned char> host(bytes);
+  double* hp = reinterpret_cast<double*>(host.data());
+  double* hk = hp + 8 * m;
+  int32_t* hput = reinterpret_cast<int32_t*>(host.data() + pbytes);
+  int64_t row = 0;
+  for (int32_t c = 0; c < n; ++c) {
+    const FpeContract& k = contracts[c];
+    const bool euro = k.option_type == 8 || k.option_type == 9;
+    const bool valid = k.kappa > 0 && k.theta > 0 && k.sigma > 0 && k.T > 0 && k.S0 > 0 &&
+                       k.V0 >= 0 && k.rho >= -1 && k.rho <= 1 && std::isfinite(k.r);
+    for (int32_t j = 0; j < k.n_strikes; ++j, ++row) {
+      const double pr[8] = {k.kappa, k.theta, k.sigma, k.rho, k.r, k.T, k.S0, k.V0};
+      std::memcpy(hp + 8 * row, pr, sizeof(pr));
+      hk[row] = k.strikes[j];
+      hput[row] = k.option_type == 9;
+      if (!euro) {
+        st[row] = FPE_STATUS_UNSUPPORTED;
+        hp[8 * row] = -1.0;  // the kernel answers NaN for a non-positive kappa
+      } else if (!valid || !(k.strikes[j] > 0.0)) {
+        st[row] = FPE_STATUS_INVALID;
+      }
+    }
+  }
+  cudaStream_t s = C.stream;
+  void* dev = nullptr;
+  const size_t out_off = (bytes + 7) & ~size_t(7);
+  CK(cudaMallocAsync(&dev, out_off + size_t(m) * sizeof(double), s));
+  unsigned char* d = static_cast<unsigned char*>(dev);
+  double* dout = reinterpret_cast<double*>(d + out_off);
+  int rc = 0;
+  if (cudaMemcpyAsync(d, host.data(), bytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      launch_cf(reinterpret_cast<double*>(d), reinterpret_cast<double*>(d) + 8 * m,
+                reinterpret_cast<int32_t*>(d + pbytes), int32_t(m), dout, s) != 0 ||
+      cudaMemcpyAsync(prices, dout, size_t(m) * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    rc = -1;
+  cudaFreeAsync(dev, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) rc = -1;
+  if (rc) return rc;
+  int worst = 0;
+  for (int64_t i = 0; i < m; ++i) {
+    if (st[i] == FPE_STATUS_OK && !std::isfinite(prices[i])) st[i] = FPE_STATUS_NONFINITE;
+    if (st[i] != FPE_STATUS_OK) prices[i] = std::nan("");
+    if (status) status[i] = st[i];
+    if (st[i] && !worst) worst = st[i];
   }
   return worst;
 }

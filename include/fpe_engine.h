@@ -254,6 +254,30 @@ extern int32_t fpe_device_available(void);
 extern int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatchOptions* opt,
                                  double* prices, int32_t* status, void* cuda_stream);
 
+/** European prices from the Heston characteristic function (Heston 1993
+ *  probabilities in the Albrecher et al. 2007 form, composite 16-point
+ *  Gauss-Legendre quadrature), FP64, one warp per price.
+ *
+ *  No counterpart in the reference, which has no closed-form price; it
+ *  measures the discretization error of the FPE prices of Europeans and prices
+ *  European quotes directly.  Device pointers: params_dev holds n rows of 8
+ *  values (kappa, theta, sigma, rho, r, T, S0, V0), strikes_dev n strikes,
+ *  put_dev n flags (non-zero: put by put-call parity; NULL: all calls);
+ *  prices_dev receives n prices, NaN for a row outside the model's domain.
+ *  Asynchronous on cuda_stream (NULL: the library's stream).  Returns 0, or
+ *  < 0 on a bad argument or CUDA error. */
+extern int32_t fpe_heston_cf_batch(const double* params_dev, const double* strikes_dev,
+                                   const int32_t* put_dev, int32_t n, double* prices_dev,
+                                   void* cuda_stream);
+
+/** The same prices for host contracts, one per strike in contract order like
+ *  fpe_price_batch (grid fields are ignored).  Option types 8 (call) and 9
+ *  (put) only: other types get FPE_STATUS_UNSUPPORTED, invalid parameters
+ *  FPE_STATUS_INVALID, and NaN prices.  Synchronous; returns 0, the first
+ *  non-zero status, or < 0 on a bad argument or CUDA error. */
+extern int32_t fpe_heston_cf_price(const FpeContract* contracts, int32_t n, double* prices,
+                                   int32_t* status);
+
 #ifdef __cplusplus
 }
 #endif

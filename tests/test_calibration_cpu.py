@@ -2,6 +2,7 @@
 src/numerics/optim/lm.mojo:29-121) and the calibrator clamps
 (src/engines/calibrator/calibrator.mojo:15-29)."""
 import numpy as np
+import pytest
 
 from fpe_option_b200.calibration import Surface, clamp, contract_tables, levenberg_marquardt
 
@@ -44,3 +45,63 @@ def test_clamps_and_contract_tables():
     assert P.shape == (12, 12) and I.shape == (12, 3)
     assert np.allclose(P[:6, 8], [90, 100, 110, 90, 100, 110]) and np.allclose(P[6:, 0], 2.0)
     assert np.all(I[:, 2] == 8)
+
+
+def _fake_backends(monkeypatch, A, sur_sign, centre, bias):
+    """Replace the FPE and surrogate back-ends by linear models over the quotes:
+    FPE prices x A^T; surrogate prices sur_sign (x - centre) A^T + centre A^T + bias."""
+    from fpe_option_b200 import calibration as cal
+
+    class FakeFpe(cal._Backend):
+        def __init__(self, surface, **kw):
+            super().__init__(surface)
+
+        def steps(self, x):
+            return 1e-6 * (1.0 + np.abs(x))
+
+        def price_sets(self, xs):
+            self.contracts_priced += len(xs) * len(self.surface.strikes)
+            return np.atleast_2d(xs) @ A.T
+
+    class FakeSur(cal._Backend):
+        @classmethod
+        def project(cls, x):
+            return np.asarray(x, np.float64)
+
+        def __init__(self, surface, pricer, grid=None):
+            super().__init__(surface)
+            self.fallback_quotes = 0
+
+        def steps(self, x):
+            return 1e-6 * (1.0 + np.abs(x))
+
+        def price_sets(self, xs):
+            xs = np.atleast_2d(xs)
+            return (sur_sign * (xs - centre) + centre) @ A.T + bias
+
+    monkeypatch.setattr(cal, "FpeSurface", FakeFpe)
+    monkeypatch.setattr(cal, "SurrogateSurface", FakeSur)
+    return cal
+
+
+class _Pricer:
+    last_spread = np.zeros(1)
+
+
+@pytest.mark.parametrize("sur_sign,expect", [(-1.0, "hybrid->fpe"), (1.0, "hybrid")])
+def test_hybrid_polish_falls_back_to_fpe_jacobians(monkeypatch, sur_sign, expect):
+    """A surrogate whose Jacobian points the wrong way (reflected model) makes
+    every hybrid step raise the FPE residual; the polish then finishes on FPE
+    Jacobians and still reaches the FPE fit.  With a faithful Jacobian the
+    hybrid polish alone gets there."""
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((15, 5))
+    truth = np.array([1.5, 0.06, 0.4, -0.5, 0.05])
+    centre = truth + np.array([0.3, 0.01, 0.05, 0.1, 0.01])
+    cal = _fake_backends(monkeypatch, A, sur_sign, centre, 0.01 * rng.standard_normal(15))
+    surf = cal.Surface.grid(100.0, 0.02, [0.9, 1.0, 1.1], [0.5, 1.0, 1.5, 2.0, 2.5])
+    surf.prices = truth @ A.T
+    x0 = truth + np.array([-0.4, 0.02, -0.1, 0.2, 0.02])
+    x, info = cal.calibrate_with_surrogate(surf, _Pricer(), x0, polish="hybrid", polish_iter=10)
+    assert info["polish"] == expect
+    assert np.abs(x - truth).max() < 1e-6, (x, truth, info)
