@@ -349,41 +349,49 @@ __device__ __forceinline__ void stage_elem(ET* dst, const ET* src) {
   }
 }
 
+// Stages block row i: with PIVOT its pivot block (into the Gauss-Jordan
+// array, and the pivot bookkeeping reset), with REST the nr U blocks of row i
+// and E blocks of column i.
 template <typename ET, bool ASYNC>
-__device__ void fac_stage_impl(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
+__device__ void fac_stage_impl(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, bool pivot, bool rest) {
   const int nv = S.nv, nn = nv * nv, w1 = S.w1, p = S.nvp, t = S.ldt;
   const float rnv = 1.0f / float(nv);
-  const ET* P = L.blk(i, 3);
-  for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-    int r, c;
-    rc_of(e, nv, rnv, r, c);
-    stage_elem<ET, ASYNC>(S.aug + r * w1 + c, P + e);
-  }
-  for (int cc = 0; cc < nr; ++cc) {
-    const ET* U = L.blk(i, 4 + cc);
-    const ET* E = L.blk(i + 1 + cc, 2 - cc);
-    ET* ub = S.Ub + cc * p * p;
-    ET* et = S.EbT + cc * p * t;
+  if (pivot) {
+    const ET* P = L.blk(i, 3);
     for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-      int j, l;
-      rc_of(e, nv, rnv, j, l);
-      stage_elem<ET, ASYNC>(ub + j * p + l, U + e);
-      stage_elem<ET, ASYNC>(et + l * t + j, E + e);
+      int r, c;
+      rc_of(e, nv, rnv, r, c);
+      stage_elem<ET, ASYNC>(S.aug + r * w1 + c, P + e);
+    }
+    for (int r = threadIdx.x; r < nv; r += blockDim.x) {
+      S.q_of[r] = r;  // stays a valid column index even if a pivot search fails
+      S.prow_of[r] = r;
     }
   }
-  for (int r = threadIdx.x; r < nv; r += blockDim.x) {
-    S.q_of[r] = r;  // stays a valid column index even if a pivot search fails
-    S.prow_of[r] = r;
+  if (rest) {
+    for (int cc = 0; cc < nr; ++cc) {
+      const ET* U = L.blk(i, 4 + cc);
+      const ET* E = L.blk(i + 1 + cc, 2 - cc);
+      ET* ub = S.Ub + cc * p * p;
+      ET* et = S.EbT + cc * p * t;
+      for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+        int j, l;
+        rc_of(e, nv, rnv, j, l);
+        stage_elem<ET, ASYNC>(ub + j * p + l, U + e);
+        stage_elem<ET, ASYNC>(et + l * t + j, E + e);
+      }
+    }
   }
   if constexpr (ASYNC) cp_async_wait_all();
 }
 
 template <typename ET>
-__device__ void fac_stage(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
+__device__ void fac_stage(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, bool pivot = true,
+                          bool rest = true) {
   if (S.shared) {
-    fac_stage_impl<ET, true>(L, S, i, nr);
+    fac_stage_impl<ET, true>(L, S, i, nr, pivot, rest);
   } else {
-    fac_stage_impl<ET, false>(L, S, i, nr);
+    fac_stage_impl<ET, false>(L, S, i, nr, pivot, rest);
   }
 }
 
@@ -520,15 +528,20 @@ __device__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
   }
 }
 
-// Schur update E_{i+1+r, i+1+c} -= L_r U_c in the factor storage (r, c < nr);
-// the target tile is loaded first so its latency overlaps the products.
-template <typename ET>
-__device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
+// Schur update E_{i+1+r, i+1+c} -= L_r U_c (r, c < nr) for the jobs
+// job_lo <= r nr + c < job_hi, by threads lt = 0 .. nt - 1 of a team; the
+// target tile is loaded first so its latency overlaps the products.  Job 0
+// (the next pivot block E_{i+1, i+1}) goes with TO_AUG into the Gauss-Jordan
+// array instead of the factor storage: the next block row inverts it from
+// there, and the factor storage of that block receives its inverse.
+template <typename ET, bool TO_AUG>
+__device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, int job_lo, int job_hi, int lt,
+                           int nt) {
   constexpr int TM = TileM<ET>::v;
   const int nv = S.nv, p = S.nvp, t = S.ldt;
   const int tr = p / TM, tc = p / kTileN, ntile = tr * tc;
-  for (int q = threadIdx.x; q < nr * nr * ntile; q += blockDim.x) {
-    const int job = q / ntile, tt = q - job * ntile;
+  for (int q = lt; q < (job_hi - job_lo) * ntile; q += nt) {
+    const int jq = q / ntile, tt = q - jq * ntile, job = job_lo + jq;
     const int j0 = (tt / tc) * TM, l0 = (tt - (tt / tc) * tc) * kTileN;
     const int rr = job / nr, cc = job - rr * nr;
     ET* E = L.blk(i + 1 + rr, cc - rr + 3);
@@ -539,11 +552,19 @@ __device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int n
       for (int n = 0; n < kTileN; ++n)
         acc[m][n] = (j0 + m < nv && l0 + n < nv) ? E[(j0 + m) * nv + l0 + n] : fzero(ET());
     tile_mm<ET, true>(S.LbT + rr * p * t, t, S.Ub + cc * p * p, p, nv, j0, l0, acc);
+    if constexpr (TO_AUG) {
 #pragma unroll
-    for (int m = 0; m < TM; ++m)
+      for (int m = 0; m < TM; ++m)
 #pragma unroll
-      for (int n = 0; n < kTileN; ++n)
-        if (j0 + m < nv && l0 + n < nv) E[(j0 + m) * nv + l0 + n] = acc[m][n];
+        for (int n = 0; n < kTileN; ++n)
+          if (j0 + m < nv && l0 + n < nv) S.aug[(j0 + m) * S.w1 + l0 + n] = acc[m][n];
+    } else {
+#pragma unroll
+      for (int m = 0; m < TM; ++m)
+#pragma unroll
+        for (int n = 0; n < kTileN; ++n)
+          if (j0 + m < nv && l0 + n < nv) E[(j0 + m) * nv + l0 + n] = acc[m][n];
+    }
   }
 }
 
@@ -553,24 +574,37 @@ __device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int n
 template <typename FT>
 __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC, FT* scr_r,
                                 Cx<FT>* scr_c, long long (&tcyc)[2]) {
-  const int ns = LR.ns, nv = LR.nv;
+  const int ns = LR.ns;
   FacScratch<FT> SR;
-  SR.init(scr_r, nv);
+  SR.init(scr_r, LR.nv);
   FacScratch<Cx<FT>> SC;
-  if (LC) SC.init(scr_c, nv);
+  if (LC) SC.init(scr_c, LR.nv);
   bool ok = true;
   const int warp = threadIdx.x >> 5;
-  for (int i = 0; i < ns; ++i) {
-    const int nr = min(i + 3, ns - 1) - i;
-    fac_stage<FT>(LR, SR, i, nr);
-    if (LC) fac_stage<Cx<FT>>(*LC, SC, i, nr);
-    __syncthreads();
-    // pivot-block inverses: warp 0 real, warp 1 complex, concurrently
+  // Lookahead: block row i computes the next pivot block first (Schur job 0,
+  // straight into the Gauss-Jordan array); warps 0 and 1 then invert it (real,
+  // complex) while warps 2.. apply row i's remaining Schur updates, so the
+  // latency-bound inversions overlap the block products.  Block row 0 stages
+  // and inverts its own pivot block.
+  const bool split = blockDim.x >= 128;
+  if (ns <= 0) return true;
+  {
     const long long t0 = clock64();
+    fac_stage<FT>(LR, SR, 0, min(3, ns - 1));
+    if (LC) fac_stage<Cx<FT>>(*LC, SC, 0, min(3, ns - 1));
+    __syncthreads();
     if (warp == 0) ok &= fac_gj_warp<FT>(SR);
     else if (warp == 1 && LC) ok &= fac_gj_warp<Cx<FT>>(SC);
     __syncthreads();
     tcyc[0] += clock64() - t0;
+  }
+  for (int i = 0; i < ns; ++i) {
+    const int nr = min(i + 3, ns - 1) - i;
+    if (i > 0) {  // U and E blocks of row i (its pivot block is already inverted)
+      fac_stage<FT>(LR, SR, i, nr, false, true);
+      if (LC) fac_stage<Cx<FT>>(*LC, SC, i, nr, false, true);
+      __syncthreads();
+    }
     fac_extract<FT>(LR, SR, i);
     if (LC) fac_extract<Cx<FT>>(*LC, SC, i);
     __syncthreads();
@@ -579,10 +613,39 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
       fac_lw<FT>(LR, SR, i, nr);
       if (LC) fac_lw<Cx<FT>>(*LC, SC, i, nr);
       __syncthreads();
-      fac_update<FT>(LR, SR, i, nr);
-      if (LC) fac_update<Cx<FT>>(*LC, SC, i, nr);
+      // the next pivot block into the Gauss-Jordan arrays; fresh bookkeeping
+      fac_update<FT, true>(LR, SR, i, nr, 0, 1, threadIdx.x, blockDim.x);
+      if (LC) fac_update<Cx<FT>, true>(*LC, SC, i, nr, 0, 1, threadIdx.x, blockDim.x);
+      for (int r = threadIdx.x; r < SR.nv; r += blockDim.x) {
+        SR.q_of[r] = r;
+        SR.prow_of[r] = r;
+        if (LC) {
+          SC.q_of[r] = r;
+          SC.prow_of[r] = r;
+        }
+      }
       __syncthreads();
-      tcyc[1] += clock64() - t2;
+      const long long t3 = clock64();
+      tcyc[1] += t3 - t2;
+      if (split) {
+        if (warp == 0) {
+          ok &= fac_gj_warp<FT>(SR);
+        } else if (warp == 1) {
+          if (LC) ok &= fac_gj_warp<Cx<FT>>(SC);
+        } else {
+          const int lt = threadIdx.x - 64, nt = blockDim.x - 64;
+          fac_update<FT, false>(LR, SR, i, nr, 1, nr * nr, lt, nt);
+          if (LC) fac_update<Cx<FT>, false>(*LC, SC, i, nr, 1, nr * nr, lt, nt);
+        }
+      } else {
+        fac_update<FT, false>(LR, SR, i, nr, 1, nr * nr, threadIdx.x, blockDim.x);
+        if (LC) fac_update<Cx<FT>, false>(*LC, SC, i, nr, 1, nr * nr, threadIdx.x, blockDim.x);
+        __syncthreads();
+        if (warp == 0) ok &= fac_gj_warp<FT>(SR);
+        else if (warp == 1 && LC) ok &= fac_gj_warp<Cx<FT>>(SC);
+      }
+      __syncthreads();
+      tcyc[0] += clock64() - t3;
     }
   }
   return __syncthreads_and(ok ? 1 : 0) != 0;  // the same verdict in every thread
@@ -784,8 +847,11 @@ __device__ __forceinline__ const ET* stage_block(const BlockLU<ET>& L, int s, in
   return (g < 3 && i + 1 + g < ns) ? L.blk(i, 4 + g) : nullptr;
 }
 
+// Issues the bulk copies of stage s.  gfence orders the factor's earlier
+// generic-proxy writes (the factorization) before the async-proxy reads; the
+// factor does not change during a sweep, so only a sweep's first issue needs it.
 template <typename FT>
-__device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s) {
+__device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s, bool gfence) {
   unsigned long long* bar = P.bar + (s & 1);
   unsigned char* dst = P.buf[s & 1];
   const int nv = S.R ? S.R->nv : S.Cf->nv;
@@ -797,7 +863,7 @@ __device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s) {
     if (S.nc > 0 && stage_block(*S.Cf, s, g)) bytes += bc;
   }
   fence_proxy_async_smem();
-  fence_proxy_async_global();
+  if (gfence) fence_proxy_async_global();
   if (bytes == 0) {
     mbar_arrive(bar);
     return;
@@ -919,12 +985,14 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
   RT* ring_c_re = ringb + S.nr * nv4;
   RT* ring_c_im = ring_c_re + nv4;
 
-  uint32_t pend = 0;  // buffers with a stage in flight (thread 0's view)
-  if (tid == 0) {
-    stage_issue<FT>(S, P, 0);
+  // the thread that issues the copies: an idle one when the roles leave one
+  const int issuer = (int(blockDim.x) - 1 >= max(nreal, cbase + (S.nc > 0 ? Gc * nv : 0))) ? int(blockDim.x) - 1 : 0;
+  uint32_t pend = 0;  // buffers with a stage in flight (the issuer's view)
+  if (tid == issuer) {
+    stage_issue<FT>(S, P, 0, true);
     pend |= 1u;
     if (nstage > 1) {
-      stage_issue<FT>(S, P, 1);
+      stage_issue<FT>(S, P, 1, false);
       pend |= 2u;
     }
   }
@@ -1014,12 +1082,12 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
       ok = false;
       break;
     }
-    if (tid == 0 && s + 2 < nstage) {
-      stage_issue<FT>(S, P, s + 2);
+    if (tid == issuer && s + 2 < nstage) {
+      stage_issue<FT>(S, P, s + 2, false);
       pend |= 1u << b;
     }
   }
-  if (!ok && tid == 0) {
+  if (!ok && tid == issuer) {
     // let copies still in flight land (bounded) before the buffers are reused
     for (int b = 0; b < 2; ++b)
       if ((pend >> b) & 1u) mbar_wait_bounded(P.bar + b, (phase >> b) & 1u, kBulkWaitLimit);
