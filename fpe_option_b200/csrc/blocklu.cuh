@@ -294,6 +294,23 @@ __device__ __forceinline__ void vst(ET* p, const ET (&v)[K]) {
   for (int q = 0; q < K; ++q) p[q] = v[q];
 }
 
+// Explicit 16-byte vector stores of a TM-element run (TM x element size is
+// 16 or 32 bytes); p must be 16-byte aligned.
+__device__ __forceinline__ void vst16(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void vst16(double* p, const double (&v)[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void vst16(Cx<float>* p, const Cx<float> (&v)[2]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0].re, v[0].im, v[1].re, v[1].im);
+}
+__device__ __forceinline__ void vst16(Cx<double>* p, const Cx<double> (&v)[2]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0].re, v[0].im);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[1].re, v[1].im);
+}
+
 __device__ __forceinline__ void ffms(float& a, float x, float y) { a = fmaf(-x, y, a); }
 __device__ __forceinline__ void ffms(double& a, double x, double y) { a = fma(-x, y, a); }
 template <typename T>
@@ -489,15 +506,20 @@ __device__ void fac_extract(const BlockLU<ET>& L, FacScratch<ET>& S, int i) {
 }
 
 // L_r = E_r P^-1 (transposed to the factor storage and to LbT) and
-// W_c = P^-1 U_c (transposed to the factor storage), r, c < nr.
+// W_c = P^-1 U_c (transposed to the factor storage), r, c < nr.  Tiles are
+// numbered with the row index j varying fastest, so that a lane's TM rows of
+// one output column are contiguous in the transposed storage: one vector
+// store each, and a warp's stores cover contiguous memory.
 template <typename ET>
 __device__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
   constexpr int TM = TileM<ET>::v;
   const int nv = S.nv, p = S.nvp, t = S.ldt;
   const int tr = p / TM, tc = p / kTileN, ntile = tr * tc;
+  const bool vec = ((nv * int(sizeof(ET))) & 15) == 0 && ((L.bs * sizeof(ET)) & 15) == 0 &&
+                   (reinterpret_cast<uintptr_t>(L.F) & 15) == 0;
   for (int q = threadIdx.x; q < 2 * nr * ntile; q += blockDim.x) {
     const int job = q / ntile, tt = q - job * ntile;
-    const int j0 = (tt / tc) * TM, l0 = (tt - (tt / tc) * tc) * kTileN;
+    const int l0 = (tt / tr) * kTileN, j0 = (tt - (tt / tr) * tr) * TM;
     ET acc[TM][kTileN];
 #pragma unroll
     for (int m = 0; m < TM; ++m)
@@ -520,11 +542,23 @@ __device__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
       tile_mm<ET, false>(S.PiT, t, S.Ub + cc * p * p, p, nv, j0, l0, acc);
       dst = L.blk(i, 4 + cc);
     }
+    if (vec && j0 + TM <= nv) {
 #pragma unroll
-    for (int m = 0; m < TM; ++m)
+      for (int n = 0; n < kTileN; ++n) {
+        if (l0 + n < nv) {
+          ET col[TM];
 #pragma unroll
-      for (int n = 0; n < kTileN; ++n)
-        if (j0 + m < nv && l0 + n < nv) dst[(l0 + n) * nv + j0 + m] = acc[m][n];
+          for (int m = 0; m < TM; ++m) col[m] = acc[m][n];
+          vst16(dst + (l0 + n) * nv + j0, col);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < TM; ++m)
+#pragma unroll
+        for (int n = 0; n < kTileN; ++n)
+          if (j0 + m < nv && l0 + n < nv) dst[(l0 + n) * nv + j0 + m] = acc[m][n];
+    }
   }
 }
 
