@@ -495,13 +495,21 @@ __device__ bool fac_gj_warp(FacScratch<ET>& S) {
 template <typename ET>
 __device__ void fac_extract(const BlockLU<ET>& L, FacScratch<ET>& S, int i) {
   const int nv = S.nv, w1 = S.w1, p = S.nvp, t = S.ldt;
+  const float rnv = 1.0f / float(nv);
   ET* g = L.blk(i, 3);
+  // k varying fastest: the transposed factor store and PiT are contiguous
   for (int e = threadIdx.x; e < nv * nv; e += blockDim.x) {
-    const int k = e / nv, l = e - k * nv;
+    int l, k;
+    rc_of(e, nv, rnv, l, k);
     const ET v = fmul(S.aug[S.prow_of[k] * w1 + S.q_of[l]], S.pinv[k]);
-    S.Pi[k * p + l] = v;
     S.PiT[l * t + k] = v;
-    g[l * nv + k] = v;  // stored transposed
+    g[e] = v;  // stored transposed: g[l nv + k]
+  }
+  // l varying fastest: Pi is contiguous
+  for (int e = threadIdx.x; e < nv * nv; e += blockDim.x) {
+    int k, l;
+    rc_of(e, nv, rnv, k, l);
+    S.Pi[k * p + l] = fmul(S.aug[S.prow_of[k] * w1 + S.q_of[l]], S.pinv[k]);
   }
 }
 
