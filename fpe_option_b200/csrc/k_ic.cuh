@@ -358,8 +358,35 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_ic(const FpeSolveDesc* __restr
     Av[e] = (dd >= 0 && dd < 7) ? ov[j * 7 + dd] : 0.0;
   }
   __syncthreads();
-  jacobi_eig(nds, As, Vs, S.cs, S.red);
-  jacobi_eig(ndv, Av, Vv, S.cs, S.red);
+  // The eigendecompositions run in shared memory when the dynamic area (sized
+  // for the ADMM iterates, not yet in use) holds both matrices and both
+  // eigenvector sets: each Jacobi round reads and writes whole rows and
+  // columns between barriers, which from the global work area costs an L2
+  // round trip per phase.  The results go back to the work area once.
+  const size_t jac_bytes = (2 * size_t(nds) * nds + 2 * size_t(ndv) * ndv) * sizeof(double);
+  if (jac_bytes <= dyn_bytes && fpe_ic_admm_bytes(nds, ndv) <= dyn_bytes) {
+    double* jAs = reinterpret_cast<double*>(ic_dyn);
+    double* jVs = jAs + nds * nds;
+    double* jAv = jVs + nds * nds;
+    double* jVv = jAv + ndv * ndv;
+    for (int e = threadIdx.x; e < nds * nds; e += blockDim.x) jAs[e] = As[e];
+    for (int e = threadIdx.x; e < ndv * ndv; e += blockDim.x) jAv[e] = Av[e];
+    __syncthreads();
+    jacobi_eig(nds, jAs, jVs, S.cs, S.red);
+    jacobi_eig(ndv, jAv, jVv, S.cs, S.red);
+    for (int e = threadIdx.x; e < nds * nds; e += blockDim.x) {
+      As[e] = jAs[e];
+      Vs[e] = jVs[e];
+    }
+    for (int e = threadIdx.x; e < ndv * ndv; e += blockDim.x) {
+      Av[e] = jAv[e];
+      Vv[e] = jVv[e];
+    }
+    __syncthreads();
+  } else {
+    jacobi_eig(nds, As, Vs, S.cs, S.red);
+    jacobi_eig(ndv, Av, Vv, S.cs, S.red);
+  }
   const double sigma = 1e-6, lamreg = 1e-6, eps_abs = 1e-8, eps_rel = 1e-8;
   double rho = 0.1;
   const double alpha = lamreg + sigma + rho;
