@@ -438,6 +438,9 @@ class BatchOptions:
     greeks: bool = False
     rel_s: float = 0.01
     rel_v: float = 0.1
+    max_step: float = 0.0    # <= 0: T/5 (the reference Pricer); > 0: absolute cap
+    first_step: float = 0.0  # 0: 1e-6 (Pricer); < 0: the Radau solver's own estimate
+    price_rule: int = 0      # 1: the calibration objective's undiscounted sum (reference disc)
 
     def to_c(self) -> _lib.FpeBatchOptions:
         o = _lib.FpeBatchOptions()
@@ -449,6 +452,7 @@ class BatchOptions:
         o.rel_s, o.rel_v = self.rel_s, self.rel_v
         o.complex_solve = self.complex_solve
         o.radau_constants = self.radau_constants
+        o.max_step, o.first_step, o.price_rule = self.max_step, self.first_step, self.price_rule
         return o
 
 

@@ -54,7 +54,8 @@ class FpeBatchOptions(C.Structure):
     _fields_ = [("disc", i32), ("precision", i32), ("num_insert", i32), ("refine", i32),
                 ("rtol", d), ("atol", d), ("ic_sigma_s", d), ("ic_sigma_v", d), ("ic_sub", i32),
                 ("greeks", i32), ("rel_s", d), ("rel_v", d), ("complex_solve", i32),
-                ("radau_constants", i32)]
+                ("radau_constants", i32), ("max_step", d), ("first_step", d),
+                ("price_rule", i32)]
 
 
 # Every symbol declared in include/*.h.

@@ -8,7 +8,7 @@ rejected step and x0.1 (floored at 1e-10) after an accepted one, stop when
 reference's clamps (src/engines/calibrator/calibrator.mojo:15-29) and a central
 finite-difference Jacobian (:64-74).
 
-Two residual back-ends price the whole surface per call:
+Residual back-ends price the whole surface per call:
 
 * ``FpeSurface``: the batched FPE solver.  A Jacobian is one GPU batch of
   11 x (number of quotes) contracts (the base point and ten perturbed
@@ -16,6 +16,10 @@ Two residual back-ends price the whole surface per call:
   reference's 1e-6: an adaptive-step solver at rtol 1e-6 changes its step
   sequence between neighbouring parameter sets, which makes 1e-6 differences
   noise.
+* ``ReferenceObjectiveSurface``: the reference calibrator's own objective
+  (an 8 x 8 reference-discretization solve per quote and its undiscounted
+  density integration) for parity with that calibrator
+  (``calibrate_reference_objective``).
 * ``SurrogateSurface``: the tensor-core MLP ensemble; a Jacobian costs
   microseconds.  Its step is 2 % of the parameter's training range, coarser
   than the BF16 rounding of the network's inputs.  Inside the loop quotes
@@ -226,6 +230,30 @@ class FpeSurface(_Backend):
         return p.reshape(len(xs), -1)
 
 
+class ReferenceObjectiveSurface(FpeSurface):
+    """Residuals of the reference calibrator's own objective
+    (src/engines/calibrator/objective.mojo:66-104), priced on the GPU.
+
+    Each quote is an FPE solve on the reference discretization with 8 x 8
+    knots and the FPEDomain default of 251 grid inserts (:94), the FPESolver
+    settings rtol 1e-5, atol 1e-7, max_step 0.02 and first_step 0, i.e. the
+    Radau solver's own first step (:86-88), and the objective's integration of
+    the terminal density: payoff max(S - K, 0) times pdf times half the
+    neighbour spacing in s and v (1 at both ends), undiscounted (:26-50).  The
+    FP64 factors, GMRES(10) stage solve and the reference's Radau constants
+    are the reference's arithmetic.  The Jacobian step is the calibrator's
+    1e-6 (1 + |x|) (calibrator.mojo:64-74).  All quotes of a residual or
+    Jacobian go to the solver as one batch."""
+
+    def __init__(self, surface: Surface, grid=(8, 8), rel_step: float = 1e-6):
+        from . import BatchOptions
+
+        opts = BatchOptions(disc=0, precision=0, num_insert=251, rtol=1e-5, atol=1e-7,
+                            complex_solve=1, radau_constants=1, max_step=0.02, first_step=-1.0,
+                            price_rule=1)
+        super().__init__(surface, options=opts, grid=grid, rel_step=rel_step)
+
+
 class SurrogateSurface(_Backend):
     """Residuals from a SurrogatePricer (FPE fall-back for untrusted quotes).
     Parameter vectors are projected into the surrogate's training box before
@@ -285,6 +313,18 @@ class HybridSurface:
     def jacobian(self, x):
         _, J = self.sur.jacobian(x)
         return self.fpe.residual(x), J
+
+
+def calibrate_reference_objective(surface: Surface, x0, max_iter=50, tol=1e-8, **kw):
+    """The reference Calibrator (calibrator.mojo:87-119): LM with lambda 1e-3,
+    x10 / x0.1 (lm.mojo:29-121) on the reference objective, the parameters
+    clamped as in _vec_to_params.  Only call quotes (option type 8) exist in
+    that objective.  Returns (x, info)."""
+    be = ReferenceObjectiveSurface(surface, **kw)
+    t = time.perf_counter()
+    res = levenberg_marquardt(be.residual, be.jacobian, x0, max_iter=max_iter, tol=tol)
+    return clamp(res.x), {"seconds": time.perf_counter() - t, "fpe_contracts": be.contracts_priced,
+                          "iterations": res.iterations, "cost": res.cost, "stop": res.stop}
 
 
 def calibrate_fpe(surface: Surface, x0, max_iter=40, tol=1e-10, **kw):

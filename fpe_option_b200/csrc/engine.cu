@@ -107,6 +107,8 @@ struct Opts {
   int radau_exact = 0;   // resolved: 0 the reference's stage constants, 1 exact Radau IIA
   double rtol = 1e-4, atol = 1e-6, ic_sigma_s = 0.6, ic_sigma_v = 0.004, rel_s = 0.01,
          rel_v = 0.1;
+  double max_step = 0.0, first_step = 0.0;  // 0: the reference Pricer's T/5 and 1e-6
+  int price_rule = 0;                       // 1: calibration-objective integration
 };
 
 Opts opts_from(const FpeBatchOptions* o, int default_num_insert) {
@@ -131,6 +133,9 @@ Opts opts_from(const FpeBatchOptions* o, int default_num_insert) {
   r.greeks = o->greeks;
   if (o->rel_s > 0) r.rel_s = o->rel_s;
   if (o->rel_v > 0) r.rel_v = o->rel_v;
+  if (o->max_step > 0) r.max_step = o->max_step;
+  r.first_step = std::isfinite(o->first_step) ? o->first_step : 0.0;
+  r.price_rule = (o->price_rule == 1 && o->disc == 0) ? 1 : 0;
   return r;
 }
 
@@ -158,6 +163,8 @@ FpeSolveDesc make_desc(const Pricing& p, int solve_type, double barrier, const O
   d.vmin = 0.0; d.vmax = 1.0;
   d.barrier = barrier;
   d.rtol = o.rtol; d.atol = o.atol;
+  d.max_step = o.max_step; d.first_step = o.first_step;
+  d.price_rule = o.price_rule;
   d.ic_sigma_s = o.ic_sigma_s; d.ic_sigma_v = o.ic_sigma_v;
   d.type = solve_type;
   d.n_s = p.n_s; d.n_v = p.n_v;

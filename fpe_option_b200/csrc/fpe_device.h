@@ -44,11 +44,14 @@ struct FpeSolveDesc {
   double smin, smax, vmin, vmax;
   double barrier;
   double rtol, atol;
+  double max_step;       // <= 0: T / 5 (the reference Pricer)
+  double first_step;     // 0: 1e-6 (Pricer); < 0: the Radau solver's estimate
   double ic_sigma_s, ic_sigma_v;
   int32_t type;          // 0..9; knock-ins are split into two solves by the host
   int32_t n_s, n_v;      // knot-count inputs
   int32_t left_neu, right_neu;
   int32_t disc;          // 0 reference, 1 config
+  int32_t price_rule;    // 1: calibration-objective integration (reference disc)
   int32_t num_insert;
   int32_t ic_sub;
   int32_t strike_off, n_strikes;

@@ -29,6 +29,7 @@ __device__ __forceinline__ double payoff_value(int type, double S, double K, dou
 struct PayoffSmem {
   double red[32 * 2];
   double r[FPE_MAX_NDOF_S];
+  double mvo[FPE_MAX_NDOF_V];  // v weights of the calibration-objective rule
 };
 
 __global__ void __launch_bounds__(FPE_BLOCK) k_payoff(const FpeSolveDesc* __restrict__ descs,
@@ -53,13 +54,36 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_payoff(const FpeSolveDesc* __rest
   const int nds = info[FPE_INFO_NDOF_S], ndv = info[FPE_INFO_NDOF_V];
   const double* qT = D + DL.qT;
   const double* mv = D + DL.m_v;
+  // The calibration objective (objective.mojo:26-50) sums payoff * pdf * ds * dv
+  // over the quadrature points with half the neighbour spacing as weight (1 at
+  // both ends) and no discount.  In reduced form its v weights are
+  // mv'_b = sum_q Bv_qb dv_q, and ds replaces the s quadrature weight below.
+  const bool objective = d.disc == 0 && d.price_rule == 1;
+  if (objective) {
+    const int nqv = info[FPE_INFO_NQ_V];
+    const double* vp = D + DL.qp_v;
+    const double* Bv = D + DL.B_v;
+    const int32_t* c0v = I + IL.c0_v;
+    for (int b = threadIdx.x; b < ndv; b += blockDim.x) {
+      double acc = 0.0;
+      for (int q = 0; q < nqv; ++q) {
+        const int t = b - c0v[q];
+        if (t < 0 || t > 3) continue;
+        const double dv = (q > 0 && q < nqv - 1) ? 0.5 * (vp[q + 1] - vp[q - 1]) : 1.0;
+        acc += Bv[4 * q + t] * dv;
+      }
+      S.mvo[b] = acc;
+    }
+    __syncthreads();
+    mv = S.mvo;
+  }
   for (int a = threadIdx.x; a < nds; a += blockDim.x) {
     double acc = 0.0;
     for (int b = 0; b < ndv; ++b) acc += qT[a * ndv + b] * mv[b];
     S.r[a] = acc;
   }
   __syncthreads();
-  const double disc = exp(-d.r * d.T);
+  const double disc = objective ? 1.0 : exp(-d.r * d.T);
   const double* ks = strikes + d.strike_off;
   if (d.disc == 0) {
     const int nq = info[FPE_INFO_NQ_S];
@@ -80,7 +104,8 @@ __global__ void __launch_bounds__(FPE_BLOCK) k_payoff(const FpeSolveDesc* __rest
           const int a = cc + s;
           if (a < nds) dot += Bt[4 * p + s] * S.r[a];
         }
-        part += pay * (dot * qw[p]);
+        const double wp = objective ? ((p > 0 && p < nq - 1) ? 0.5 * (qp[p + 1] - qp[p - 1]) : 1.0) : qw[p];
+        part += pay * (dot * wp);
       }
       const double tot = block_sum1(part, S.red);
       if (threadIdx.x == 0) prices[d.strike_off + k] = tot * disc;

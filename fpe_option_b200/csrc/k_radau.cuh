@@ -115,6 +115,26 @@ struct RadauSmem {
   int piv[4];
 };
 
+// The Radau solver's own first step (radau.mojo:168-184): 0.01 / rms(K y0 /
+// scal), or max(1e-6, 1e-3 |t1 - t0|) when that norm is tiny, capped by
+// max_step.  Out of line: it runs once per solve and stays out of the step
+// loop's register allocation.
+__device__ __noinline__ double radau_first_step(const RadauCtx& C, const KronTerm* Kt, const double* y, double* w,
+                                                double sa, double sr, double span, double max_step, double* red) {
+  const double* xi[1] = {y};
+  double* yo[1] = {w};
+  kron_apply(C, Kt, 4, xi, yo, 1);
+  double part = 0.0;
+  for (int e = threadIdx.x; e < C.N; e += blockDim.x) {
+    const double q = w[e] / (sa + sr * fabs(y[e]));
+    part += q * q;
+  }
+  const double dnf = sqrt(block_sum1(part, red) / double(C.N));
+  double h = dnf <= 1e-10 ? fmax(1e-6, span * 1e-3) : 0.01 / dnf;
+  if (max_step > 0.0) h = fmin(h, max_step);
+  return h;
+}
+
 template <typename FT>
 struct RadauKernelArgs {
   const FpeSolveDesc* descs;
@@ -333,10 +353,16 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
   const double rtol_w = 0.1 * pow(d.rtol, 2.0 / 3.0);
   const double atol_w = rtol_w * (d.atol / d.rtol);
   const double fnewt = fmax(10.0 * uround / rtol_w, fmin(0.03, sqrt(rtol_w)));
-  const double max_step = d.T / 5.0;
+  // the reference Pricer: max_step T/5, first_step 1e-6 (pricer.mojo:131-136)
+  const double max_step = d.max_step > 0.0 ? d.max_step : d.T / 5.0;
   const double sa = fmax(atol_w, 1e-300), sr = fmax(rtol_w, 1e-300);
   double t = t0;
-  double h = 1e-6;  // first_step (pricer.mojo:131-136)
+  double h = 1e-6;
+  if (d.first_step > 0.0) {
+    h = d.first_step;
+  } else if (d.first_step < 0.0) {
+    h = radau_first_step(C, Kt, y, w, sa, sr, fabs(t1 - t0), max_step, S.red);
+  }
   h = fmin(h, fabs(t1 - t0));
   h = posneg * h;
   long n_steps = 0, n_acc = 0, n_rej = 0, n_newton = 0, n_gmres = 0, n_lu = 0;

@@ -164,6 +164,15 @@ typedef struct FpeBatchOptions {
     int32_t radau_constants; /* Radau IIA stage constants: 0 auto (the reference's
                                 U1/ALPH/BETA/TI13 for disc 0, exact for disc 1),
                                 1 the reference's, 2 exact (order-5 Radau IIA) */
+    double max_step;     /* Radau step cap: <= 0 -> T/5 (the reference Pricer), > 0 absolute */
+    double first_step;   /* first Radau step: 0 -> 1e-6 (the reference Pricer); < 0 -> the
+                            solver's own estimate 0.01 / ||K y0 / scal|| (reference FPESolver
+                            with first_step 0, src/numerics/ode/radau.mojo:168-184) */
+    int32_t price_rule;  /* reference discretization only: 0 the Pricer's discounted
+                            quadrature sum (pricer.mojo:27-64); 1 the calibration
+                            objective's undiscounted sum over the quadrature points with
+                            half-spacing weights, 1 at both ends
+                            (src/engines/calibrator/objective.mojo:26-50) */
 } FpeBatchOptions;
 
 /** Status codes written per strike slot of a batch. */

@@ -437,6 +437,9 @@ struct Options {
   int ic_sub = 8;
   bool complex_direct = false;
   bool radau_exact = false;
+  double max_step = 0.0;    // <=0: T/5
+  double first_step = 0.0;  // 0: 1e-6; <0: the solver's estimate
+  int price_rule = 0;
 };
 
 static Options options_from(const OrcOptions* o, int default_num_insert) {
@@ -454,6 +457,9 @@ static Options options_from(const OrcOptions* o, int default_num_insert) {
   r.complex_direct = o->complex_direct != 0;
   // 0 auto: reference constants on the reference discretization, exact on config
   r.radau_exact = o->radau_constants == 2 || (o->radau_constants == 0 && o->disc == 1);
+  r.max_step = o->max_step;
+  r.first_step = o->first_step;
+  r.price_rule = o->price_rule;
   return r;
 }
 
@@ -1609,7 +1615,12 @@ struct Pipeline {
       }
     Vec y0(N);
     for (int i = 0; i < N; ++i) y0[i] = D[i] * q0[i];
-    RadauSolver rs{opt.rtol, opt.atol, h.T / 5.0, 1e-6, true, opt.complex_direct};
+    // Pricer: max_step T/5, first_step 1e-6 (pricer.mojo:131-136); FPESolver
+    // callers (the calibration objective, objective.mojo:86-88) pass their own,
+    // first_step 0 meaning the solver's estimate (radau.mojo:168-184)
+    const double max_step = opt.max_step > 0.0 ? opt.max_step : h.T / 5.0;
+    const double first_step = opt.first_step > 0.0 ? opt.first_step : (opt.first_step < 0.0 ? 0.0 : 1e-6);
+    RadauSolver rs{opt.rtol, opt.atol, max_step, first_step, true, opt.complex_direct};
     if (opt.radau_exact) rs.set_exact();
     sol = rs.solve(Ms, Ks, y0, h.T);
     traj.clear();
@@ -1640,6 +1651,33 @@ struct Pipeline {
       if (type == 6 || type == 7) return S < barrier;
       return true;
     };
+    if (opt.disc == 0 && opt.price_rule == 1) {
+      // calibration objective (objective.mojo:26-50): sum over the quadrature
+      // points of payoff * pdf * ds * dv, ds / dv half the neighbour spacing
+      // (1 at both ends), no discount
+      ensure_pdf();
+      size_t nqs = dom.s_phys.size(), nqv = dom.v_phys.size();
+      for (size_t k = 0; k < K.size(); ++k) {
+        double price = 0.0;
+        for (size_t i = 0; i < nqs; ++i) {
+          double S = dom.s_phys[i];
+          double ds = 1.0;
+          if (i > 0 && i < nqs - 1) ds = 0.5 * (dom.s_phys[i + 1] - dom.s_phys[i - 1]);
+          double v = 0.0;
+          if (active(S)) {
+            v = is_call ? S - K[k] : K[k] - S;
+            if (!(v > 0.0)) v = 0.0;
+          }
+          for (size_t j = 0; j < nqv; ++j) {
+            double dv = 1.0;
+            if (j > 0 && j < nqv - 1) dv = 0.5 * (dom.v_phys[j + 1] - dom.v_phys[j - 1]);
+            price += v * pdf[i * nqv + j] * ds * dv;
+          }
+        }
+        out[k] = price;
+      }
+      return out;
+    }
     if (opt.disc == 0) {
       ensure_pdf();
       size_t nqs = dom.s_w.size(), nqv = dom.v_w.size();

@@ -38,6 +38,12 @@ typedef struct OrcOptions {
     int32_t complex_direct; /* 1: exact complex stage solve instead of GMRES(10) */
     int32_t radau_constants; /* 0 auto (reference for disc 0, exact for disc 1),
                                 1 the reference's U1/ALPH/BETA, 2 exact Radau IIA */
+    double max_step;       /* <=0 -> T/5 (Pricer, pricer.mojo:131-136); >0 absolute */
+    double first_step;     /* 0 -> 1e-6 (Pricer); <0 -> the solver's own estimate
+                              (radau.mojo:168-184, FPESolver first_step=0); >0 as given */
+    int32_t price_rule;    /* reference disc: 0 Pricer._price_at (discounted quadrature
+                              sum); 1 the calibration objective's undiscounted sum with
+                              half-spacing weights (objective.mojo:26-50) */
 } OrcOptions;
 
 /* ComputePipeline(fp, num_insert) (reference src/server/compute_pipeline.mojo:29-48).

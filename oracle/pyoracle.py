@@ -30,6 +30,9 @@ class OrcOptions(C.Structure):
         ("ic_sub", C.c_int32),
         ("complex_direct", C.c_int32),
         ("radau_constants", C.c_int32),
+        ("max_step", C.c_double),
+        ("first_step", C.c_double),
+        ("price_rule", C.c_int32),
     ]
 
 
@@ -90,9 +93,10 @@ def _dp(a: np.ndarray):
 
 
 def options(disc=0, num_insert=0, rtol=0.0, atol=0.0, ic_sigma_s=0.0, ic_sigma_v=0.0,
-            nnls_exact=0, ic_sub=0, complex_direct=0, radau_constants=0) -> OrcOptions:
+            nnls_exact=0, ic_sub=0, complex_direct=0, radau_constants=0, max_step=0.0,
+            first_step=0.0, price_rule=0) -> OrcOptions:
     return OrcOptions(disc, num_insert, rtol, atol, ic_sigma_s, ic_sigma_v, nnls_exact, ic_sub,
-                      complex_direct, radau_constants)
+                      complex_direct, radau_constants, max_step, first_step, price_rule)
 
 
 _ARRAYS = {"s_knots": 0, "v_knots": 1, "s": 2, "v": 3, "s_weights": 4, "v_weights": 5,
