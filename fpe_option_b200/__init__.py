@@ -34,7 +34,7 @@ _logger = logging.getLogger("fpe_engine")
 __all__ = [
     "price", "Compute", "FpeParams", "PriceResult", "KnotsResult", "GridPointsResult",
     "Basis1DResult", "GreeksResult", "is_available", "price_batch", "Plan", "Contract",
-    "BatchOptions", "OPTION_TYPES", "heston_cf_price",
+    "BatchOptions", "OPTION_TYPES", "heston_cf_price", "interpolate_pdf",
 ]
 
 # python/fpe_engine/__init__.py:54-60
@@ -376,6 +376,12 @@ class Compute:
                 self._L.fpe_compute_free_mat(C.byref(r))
         return self._pdf_cache
 
+    def pdf_interpolate(self, s, v) -> np.ndarray:
+        """The terminal density at points (s, v), interpolated from the pdf grid
+        (Catmull-Rom bicubic; reference src/server/interpolator.mojo)."""
+        g = self.grid_points
+        return interpolate_pdf(g.s, g.v, self.pdf, s, v)
+
     def payoff_price(self, K) -> np.ndarray:
         k = np.ascontiguousarray(_strikes(K), dtype=np.float64)
         r = _lib.FpeVecResult()
@@ -581,3 +587,32 @@ def heston_cf_price(params: np.ndarray, ints: np.ndarray):
     if rc < 0:
         raise RuntimeError("fpe_heston_cf_price failed")
     return prices, status
+
+
+def interpolate_pdf(s_points, v_points, pdf, s, v) -> np.ndarray:
+    """A density tabulated on the grid s_points x v_points (row-major pdf, e.g.
+    ``Compute.pdf`` on ``Compute.grid_points``) interpolated at the points
+    (s, v) on the GPU: Catmull-Rom bicubic, bilinear for grids with fewer than
+    4 points per axis (reference src/server/interpolator.mojo:62-198)."""
+    L = _require()
+    import torch
+
+    sp = np.ascontiguousarray(s_points, np.float64)
+    vp = np.ascontiguousarray(v_points, np.float64)
+    f = np.ascontiguousarray(pdf, np.float64)
+    sq = np.ascontiguousarray(np.atleast_1d(s), np.float64)
+    vq = np.ascontiguousarray(np.atleast_1d(v), np.float64)
+    if f.shape != (len(sp), len(vp)) or sq.shape != vq.shape:
+        raise ValueError("interpolate_pdf: pdf must be len(s_points) x len(v_points), s and v of equal length")
+    n = len(sq)
+    if n == 0:
+        return np.zeros(0)
+    dev = torch.device("cuda")
+    t = [torch.from_numpy(a).to(dev) for a in (sp, vp, f, sq, vq)]
+    out = torch.empty(n, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream or 1  # 1: the legacy default stream
+    rc = L.fpe_pdf_interpolate(t[0].data_ptr(), len(sp), t[1].data_ptr(), len(vp), t[2].data_ptr(),
+                               t[3].data_ptr(), t[4].data_ptr(), n, out.data_ptr(), stream)
+    if rc != 0:
+        raise RuntimeError("fpe_pdf_interpolate failed")
+    return out.cpu().numpy()

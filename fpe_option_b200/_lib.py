@@ -68,6 +68,7 @@ EXPORTED = [
     "fpe_plan_stats", "fpe_plan_sizes", "fpe_plan_destroy", "fpe_price_batch",
     "fpe_compute_create_ex", "fpe_compute_basis_csr", "fpe_device_available",
     "fpe_plan_kernel_times", "fpe_price_noalloc", "fpe_heston_cf_batch", "fpe_heston_cf_price",
+    "fpe_pdf_interpolate",
     # include/fpe_surrogate.h
     "fpe_mlp_create", "fpe_mlp_destroy", "fpe_mlp_layout", "fpe_mlp_get_params",
     "fpe_mlp_set_params", "fpe_mlp_forward", "fpe_mlp_train_step", "fpe_mlp_gradient",
@@ -155,5 +156,7 @@ def load():
     L.fpe_heston_cf_batch.argtypes = [vp, vp, vp, i32, vp, vp]
     L.fpe_heston_cf_price.restype = i32
     L.fpe_heston_cf_price.argtypes = [C.POINTER(FpeContract), i32, dp, ip]
+    L.fpe_pdf_interpolate.restype = i32
+    L.fpe_pdf_interpolate.argtypes = [vp, i32, vp, i32, vp, vp, vp, i32, vp, vp]
     _lib = L
     return L

@@ -23,6 +23,7 @@
 #include "k_cf.cuh"
 #include "k_galerkin.cuh"
 #include "k_ic.cuh"
+#include "k_interp.cuh"
 #include "k_payoff.cuh"
 #include "k_radau.cuh"
 #include "k_setup.cuh"
@@ -1358,4 +1359,24 @@ extern "C" int32_t fpe_heston_cf_price(const FpeContract* contracts, int32_t n, 
     if (st[i] && !worst) worst = st[i];
   }
   return worst;
+}
+
+// --------------------------------------------------------------------------
+// Terminal-density interpolation (k_interp.cuh)
+// --------------------------------------------------------------------------
+extern "C" int32_t fpe_pdf_interpolate(const double* s_points_dev, int32_t n_s, const double* v_points_dev,
+                                       int32_t n_v, const double* pdf_dev, const double* s_dev,
+                                       const double* v_dev, int32_t n, double* out_dev, void* cuda_stream) {
+  if (n < 0 || n_s < 2 || n_v < 2) return -1;
+  if (n == 0) return 0;
+  if (!s_points_dev || !v_points_dev || !pdf_dev || !s_dev || !v_dev || !out_dev) return -1;
+  Context& C = ctx();
+  if (!C.ok) return -1;
+  cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : C.stream;
+  const int block = 256;
+  const unsigned grid = unsigned((int64_t(n) + block - 1) / block);
+  fpe::k_pdf_interp<<<grid, block, 0, st>>>(s_points_dev, n_s, v_points_dev, n_v, pdf_dev, s_dev, v_dev, n,
+                                            out_dev);
+  CK(cudaGetLastError());
+  return 0;
 }

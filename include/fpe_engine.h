@@ -287,6 +287,22 @@ extern int32_t fpe_heston_cf_batch(const double* params_dev, const double* strik
 extern int32_t fpe_heston_cf_price(const FpeContract* contracts, int32_t n, double* prices,
                                    int32_t* status);
 
+/** Terminal density interpolated at n points (s, v), FP64, one thread per
+ *  point: Catmull-Rom bicubic on the 4 x 4 neighbourhood of the enclosing
+ *  cell (indices clamped at the edges, local coordinates clamped to [0, 1]),
+ *  bilinear when either axis has fewer than 4 points.
+ *
+ *  Replaces reference Interpolator.interpolate / interpolate_batch
+ *  (src/server/interpolator.mojo:62-198), which has no entry point of its
+ *  own in the reference API.  Device pointers: the grid axes (nondecreasing,
+ *  n_s and n_v >= 2), the density row-major n_s x n_v (as fpe_compute_pdf
+ *  returns it, on the points of fpe_compute_grid_points), the query
+ *  coordinates and out (n values).  Asynchronous on cuda_stream (NULL: the
+ *  library's stream).  Returns 0, or < 0 on a bad argument or CUDA error. */
+extern int32_t fpe_pdf_interpolate(const double* s_points_dev, int32_t n_s, const double* v_points_dev,
+                                   int32_t n_v, const double* pdf_dev, const double* s_dev,
+                                   const double* v_dev, int32_t n, double* out_dev, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

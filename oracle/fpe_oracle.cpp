@@ -2197,3 +2197,59 @@ int32_t orc_radau_dense(int32_t n, const double* M, const double* K, const doubl
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// PDF interpolation (src/server/interpolator.mojo:14-198): Catmull-Rom bicubic
+// on the 4 x 4 neighbourhood, bilinear below 4 points per axis.
+// ---------------------------------------------------------------------------
+static int interp_find_interval(const double* p, int n, double x) {  // :44-60, linear scan
+  if (n <= 1) return 0;
+  if (x <= p[0]) return 0;
+  if (x >= p[n - 1]) return n - 2;
+  for (int i = 0; i < n - 1; ++i)
+    if (x >= p[i] && x < p[i + 1]) return i;
+  return n - 2;
+}
+
+static void interp_cr_weights(double t, double* w) {  // :13-30
+  double t2 = t * t, t3 = t2 * t;
+  w[0] = -0.5 * t3 + t2 - 0.5 * t;
+  w[1] = 1.5 * t3 - 2.5 * t2 + 1.0;
+  w[2] = -1.5 * t3 + 2.0 * t2 + 0.5 * t;
+  w[3] = 0.5 * t3 - 0.5 * t2;
+}
+
+int32_t orc_pdf_interpolate(const double* sp, int32_t n_s, const double* vp, int32_t n_v, const double* pdf,
+                            const double* s, const double* v, int32_t n, double* out) {
+  if (n_s < 2 || n_v < 2 || n < 0) return -1;
+  auto local = [](const double* p, int i, double x) {
+    double t = 0.0;
+    if (p[i + 1] > p[i]) t = (x - p[i]) / (p[i + 1] - p[i]);
+    if (t < 0.0) t = 0.0;
+    if (t > 1.0) t = 1.0;
+    return t;
+  };
+  for (int k = 0; k < n; ++k) {
+    int i = interp_find_interval(sp, n_s, s[k]), j = interp_find_interval(vp, n_v, v[k]);
+    double ts = local(sp, i, s[k]), tv = local(vp, j, v[k]);
+    if (n_s >= 4 && n_v >= 4) {  // :125-173
+      double ws[4], wv[4];
+      interp_cr_weights(ts, ws);
+      interp_cr_weights(tv, wv);
+      double result = 0.0;
+      for (int di = 0; di < 4; ++di) {
+        int ii = std::min(std::max(i - 1 + di, 0), n_s - 1);
+        for (int dj = 0; dj < 4; ++dj) {
+          int jj = std::min(std::max(j - 1 + dj, 0), n_v - 1);
+          result += ws[di] * wv[dj] * pdf[size_t(ii) * n_v + jj];
+        }
+      }
+      out[k] = result;
+    } else {  // :77-123
+      double f00 = pdf[size_t(i) * n_v + j], f10 = pdf[size_t(i + 1) * n_v + j];
+      double f01 = pdf[size_t(i) * n_v + j + 1], f11 = pdf[size_t(i + 1) * n_v + j + 1];
+      out[k] = (1.0 - ts) * (1.0 - tv) * f00 + ts * (1.0 - tv) * f10 + (1.0 - ts) * tv * f01 + ts * tv * f11;
+    }
+  }
+  return 0;
+}

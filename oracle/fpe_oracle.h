@@ -107,6 +107,11 @@ int32_t orc_price_batch(int32_t n, const double* params, const int32_t* ints,
 
 /* FP64 Heston characteristic-function European price (Albrecher et al. 2007
  * "little Heston trap" form), Gauss-Legendre on a truncated integration range. */
+/* Interpolator.interpolate over n points (src/server/interpolator.mojo:62-198):
+ * Catmull-Rom bicubic, bilinear below 4 points per axis; pdf row-major n_s x n_v. */
+int32_t orc_pdf_interpolate(const double* s_points, int32_t n_s, const double* v_points, int32_t n_v,
+                            const double* pdf, const double* s, const double* v, int32_t n, double* out);
+
 double orc_heston_cf_price(double kappa, double theta, double sigma, double rho,
                            double r, double T, double S0, double V0, double K,
                            int32_t is_call);

@@ -74,6 +74,8 @@ def lib():
         L.orc_engine_price.argtypes = [d] * 8 + [i32, i32, d, i32, d, d, dp, i32, op, dp, dp, dp, dp]
         L.orc_price_batch.restype = i32
         L.orc_price_batch.argtypes = [i32, dp, ip, op, i32, dp]
+        L.orc_pdf_interpolate.restype = C.c_int32
+        L.orc_pdf_interpolate.argtypes = [dp, C.c_int32, dp, C.c_int32, dp, dp, dp, C.c_int32, dp]
         L.orc_heston_cf_price.restype = d
         L.orc_heston_cf_price.argtypes = [d] * 9 + [i32]
         L.orc_bspline_value.restype = d
@@ -226,3 +228,16 @@ def radau_dense(M, K, y0, t1, rtol, atol, max_step=0.0, first_step=0.0, exact=Fa
     n = lib().orc_radau_dense(len(y0), _dp(M), _dp(K), _dp(y0), t1, rtol, atol, max_step,
                               first_step, int(exact), _dp(out))
     return out, n
+
+
+def pdf_interpolate(s_points, v_points, pdf, s, v) -> np.ndarray:
+    sp = np.ascontiguousarray(s_points, np.float64)
+    vp = np.ascontiguousarray(v_points, np.float64)
+    f = np.ascontiguousarray(pdf, np.float64)
+    sq = np.ascontiguousarray(np.atleast_1d(s), np.float64)
+    vq = np.ascontiguousarray(np.atleast_1d(v), np.float64)
+    out = np.empty(len(sq))
+    rc = lib().orc_pdf_interpolate(_dp(sp), len(sp), _dp(vp), len(vp), _dp(f), _dp(sq), _dp(vq), len(sq), _dp(out))
+    if rc != 0:
+        raise ValueError("orc_pdf_interpolate: bad arguments")
+    return out
