@@ -9,7 +9,9 @@
 // Here A = As (x) Av is Kronecker, so the KKT matrix As^2 (x) Av^2 + alpha I
 // is diagonalised by the eigenvectors of As and Av (cyclic Jacobi on the
 // device); each ADMM x-update is four small dense products instead of a
-// sparse LU solve.  The iteration itself is the reference's.
+// sparse LU solve.  On the reference discretization the iteration is the
+// reference's; the config discretization adds residual balancing of rho and
+// over-relaxation (both below).
 #pragma once
 #include "dev_common.cuh"
 
@@ -476,14 +478,19 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_ic(const FpeSolveDesc* __restr
     __syncthreads();
     cta_gemm24(nds, ndv, ndv, st1, ndv, 1, sVvT, ndv, sx, ndv, nullptr, vec_v);  // (Vs X) Vv^T
     __syncthreads();
+    // Config discretization: over-relaxation x^ = a x + (1 - a) z_old,
+    // a = 1.6 (Boyd et al. 2011, sec. 3.4.3; the OSQP default), in the z and
+    // u updates; the residuals use the unrelaxed x.  The reference
+    // discretization keeps the reference's unrelaxed iteration.
     double nr[5] = {0, 0, 0, 0, 0};
     for (int e = threadIdx.x; e < N; e += blockDim.x) {
       const double xe = sx[e];
-      double zn = xe + su[e];
-      if (zn < 0.0) zn = 0.0;
       const double zo = sz[e];
+      const double xh = d.disc == 1 ? 1.6 * xe + (1.0 - 1.6) * zo : xe;
+      double zn = xh + su[e];
+      if (zn < 0.0) zn = 0.0;
       sz[e] = zn;
-      const double un = su[e] + xe - zn;
+      const double un = su[e] + xh - zn;
       su[e] = un;
       const double pv = xe - zn, dv = rho * (zn - zo);
       nr[0] += pv * pv;

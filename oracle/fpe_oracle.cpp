@@ -869,6 +869,11 @@ static Vec nnls_admm(const CSR& M, const Vec& b, long* iters, bool adaptive = fa
   Vec q(n);
   Mt.spmv(b.data(), q.data());
   Vec x(n, 0.0), z(n, 0.0), z_old(n, 0.0), u(n, 0.0), rhs(n);
+  // Config discretization: over-relaxation x^ = a x + (1 - a) z_old with
+  // a = 1.6 (Boyd et al. 2011, sec. 3.4.3; the OSQP default) in the z and u
+  // updates; the residuals use the unrelaxed x.  The reference
+  // discretization keeps the reference's unrelaxed iteration.
+  const double relax = adaptive ? 1.6 : 1.0;
   long it = 0;
   for (it = 0; it < max_iter; ++it) {
     for (int i = 0; i < n; ++i) rhs[i] = q[i] + rho * (z[i] - u[i]) + sigma * x[i];
@@ -877,10 +882,11 @@ static Vec nnls_admm(const CSR& M, const Vec& b, long* iters, bool adaptive = fa
     z_old = z;
     double pr = 0, du = 0, zn = 0, xn = 0, un = 0;
     for (int j = 0; j < n; ++j) {
-      double zn_ = x[j] + u[j];
+      const double xh = adaptive ? relax * x[j] + (1.0 - relax) * z_old[j] : x[j];
+      double zn_ = xh + u[j];
       if (zn_ < 0.0) zn_ = 0.0;
       z[j] = zn_;
-      u[j] = u[j] + x[j] - zn_;
+      u[j] = u[j] + xh - zn_;
       double pv = x[j] - zn_;
       pr += pv * pv;
       double dv = rho * (zn_ - z_old[j]);
