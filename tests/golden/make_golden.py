@@ -40,7 +40,7 @@ def main():
                     option_type=int(8 + k % 2), n_s=10, n_v=10)
         p = po.pricer_price(**args, opt=po.options(num_insert=50))
         cases.append({"args": args, "options": {"num_insert": 50}, "prices": p.tolist()})
-    # config discretization, tight tolerances (config-0 style, small grids)
+    # config discretization, tight tolerances (single contracts on small grids)
     for k in range(4):
         args = dict(kappa=float(rng.uniform(0.5, 3)), theta=float(rng.uniform(0.02, 0.15)),
                     sigma=float(rng.uniform(0.1, 0.8)), rho=float(rng.uniform(-0.9, 0)),

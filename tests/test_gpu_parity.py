@@ -251,8 +251,8 @@ def test_stepwise_invalid_and_domain(engine):
     assert len(pr.prices) == 3 and isinstance(pr, fpe.PriceResult)
 
 
-def test_config0_single_contract(engine, oracle):
-    """The single plain FP64 contract of the config-0 workload: S0 60, V0 0.1,
+def test_single_contract_40x24_tight_tolerance(engine, oracle):
+    """A single plain FP64 contract at tight tolerance: S0 60, V0 0.1,
     r 0.1, kappa 1.2, theta 0.05, eta 0.35, rho -0.4, T 0.6, call K 60 on
     [0, 180] x [0, 1], 40 x 24 sinh knots, 4-point Gauss-Legendre per span,
     IC sigma (0.6, 0.004), rtol 1e-8, atol 1e-10.  The device solve matches the
@@ -271,5 +271,5 @@ def test_config0_single_contract(engine, oracle):
         assert st[0] == 0
         assert abs(got[0] - ref[0]) <= tol * abs(ref[0]), (prec, got, ref)
     cf = oracle.heston_cf(1.2, 0.05, 0.35, -0.4, 0.1, 0.6, 60.0, 0.1, 60.0, True)
-    print("config-0 price %.8f oracle %.8f CF %.8f rel disc. err %.2e" % (got[0], ref[0], cf, abs(got[0] - cf) / cf))
+    print("single-contract price %.8f oracle %.8f CF %.8f rel disc. err %.2e" % (got[0], ref[0], cf, abs(got[0] - cf) / cf))
     assert abs(got[0] - cf) / cf < 2e-2
