@@ -143,3 +143,24 @@ def test_dropin_import_alias():
 
     assert hasattr(fpe_engine, "price") and hasattr(fpe_engine, "Compute")
     assert fpe_engine.Compute.__name__ == "Compute"
+
+
+@pytest.mark.parametrize("cname", ["FpeContract", "FpeBatchOptions"])
+def test_batch_struct_layouts_match_the_header(tmp_path, cname):
+    """The ctypes mirrors of the batch structs have the C header's size and
+    field offsets (a field added to one side only would shift the rest)."""
+    import subprocess
+
+    from fpe_option_b200 import _lib
+
+    st = getattr(_lib, cname)
+    fields = [f[0] for f in st._fields_]
+    body = "".join(f'  printf("%zu\\n", offsetof({cname}, {f}));\n' for f in fields)
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "fpe_engine.h"\n'
+                   f"int main(void) {{\n  printf(\"%zu\\n\", sizeof({cname}));\n{body}  return 0;\n}}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert out[0] == C.sizeof(st)
+    assert out[1:] == [getattr(st, f).offset for f in fields]
