@@ -273,3 +273,23 @@ def test_single_contract_40x24_tight_tolerance(engine, oracle):
     cf = oracle.heston_cf(1.2, 0.05, 0.35, -0.4, 0.1, 0.6, 60.0, 0.1, 60.0, True)
     print("single-contract price %.8f oracle %.8f CF %.8f rel disc. err %.2e" % (got[0], ref[0], cf, abs(got[0] - cf) / cf))
     assert abs(got[0] - cf) / cf < 2e-2
+
+
+def test_global_scratch_factorization_matches_oracle(engine, oracle):
+    """A grid whose FP32 factorization scratch exceeds shared memory (48
+    v-dofs: 352 KB for the real and complex FP32 pivot-block arrays) runs the
+    global-memory scratch path (plain staging loads, the same lookahead
+    factorization, unstaged sweeps); the small grid of the same batch keeps
+    shared memory.  Mixed precision against the FP64 oracle on the same
+    discretization, at the Radau tolerance's scale."""
+    fpe = engine
+    P = np.array([[1.2, 0.05, 0.35, -0.4, 0.1, 0.6, 60.0, 0.1, 60.0, 0.0, 0.0, 180.0],
+                  [1.2, 0.05, 0.35, -0.4, 0.1, 0.6, 60.0, 0.1, 62.0, 0.0, 0.0, 180.0]])
+    I = np.array([[24, 48, 8], [24, 16, 9]], np.int32)
+    opts = fpe.BatchOptions(disc=1, precision=1, rtol=1e-6, atol=1e-8, complex_solve=2, radau_constants=2)
+    got, st = fpe.price_batch(P, I, opts)
+    assert (st == 0).all()
+    ref = oracle.price_batch(P, I, oracle.options(disc=1, rtol=1e-6, atol=1e-8, complex_direct=1,
+                                                  radau_constants=2), n_threads=2)
+    print("global-scratch path", got, "oracle", ref)
+    np.testing.assert_allclose(got, ref, rtol=2e-5)
