@@ -120,12 +120,17 @@ FPE_HD int fpe_fac_scratch_elems(int nv) {
 }
 
 // Shared memory of the IC projection's ADMM (bytes): eigenvector matrices
-// Vs (nds^2), Vv and Vv^T (ndv^2 each), the five iterates, lam and q (N each),
-// every section rounded to an even number of doubles.
+// Vs (nds x (nds + 2)), Vv and Vv^T (ndv^2 each), the iterates, lam and q (N
+// each) and the intermediate (nds x (ndv + 2)), every section rounded to an
+// even number of doubles.
+// Vs and the products' intermediate have their rows padded by two doubles
+// (strides nds + 2 and ndv + 2), so the row-wise operand loads of a warp's
+// tiles fall on different banks.
 FPE_HD size_t fpe_ic_admm_bytes(int nds, int ndv) {
   auto ev = [](size_t n) { return (n + 1) & ~size_t(1); };
   const size_t N = size_t(nds) * ndv;
-  return (ev(size_t(nds) * nds) + 2 * ev(size_t(ndv) * ndv) + 7 * ev(N)) * sizeof(double);
+  return (ev(size_t(nds) * (nds + 2)) + 2 * ev(size_t(ndv) * ndv) + 6 * ev(N) + ev(size_t(nds) * (ndv + 2))) *
+         sizeof(double);
 }
 
 FPE_HD FpeDLayout fpe_dlayout(const FpeSolveDesc& d) {

@@ -426,8 +426,13 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_ic(const FpeSolveDesc* __restr
 
   // ---- ADMM (osqp.mojo:93-157) ------------------------------------------
   // Shared-memory resident when it fits: eigenvectors Vs, Vv and Vv^T, the
-  // five iterates, lam and q, each section at an even (16-byte) offset.
+  // five iterates, lam and q, each section at an even (16-byte) offset.  In
+  // shared memory the rows of Vs and of the intermediate t1 are padded by two
+  // doubles (strides lds, ldt): three of the four products read their left
+  // operand along rows, and unpadded rows of 32 or 64 doubles put a warp's
+  // four row groups on one bank.
   const size_t need = fpe_ic_admm_bytes(nds, ndv);
+  int lds = nds, ldt = ndv;
   double* sVs = Vs;
   double* sVv = Vv;
   double* sVvT = vec + 8 * size_t(N);  // global fallback: after the iterates (work area)
@@ -435,8 +440,10 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_ic(const FpeSolveDesc* __restr
   auto ev = [](int n) { return (n + 1) & ~1; };
   if (need <= dyn_bytes) {
     double* sm = reinterpret_cast<double*>(ic_dyn);
+    lds = nds + 2;
+    ldt = ndv + 2;
     sVs = sm;
-    sVv = sVs + ev(nds * nds);
+    sVv = sVs + ev(nds * lds);
     sVvT = sVv + ev(ndv * ndv);
     sx = sVvT + ev(ndv * ndv);
     sz = sx + ev(N);
@@ -444,8 +451,11 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_ic(const FpeSolveDesc* __restr
     sq = su + ev(N);
     srhs = sq + ev(N);
     st1 = srhs + ev(N);
-    slam = st1 + ev(N);
-    for (int e = threadIdx.x; e < nds * nds; e += blockDim.x) sVs[e] = Vs[e];
+    slam = st1 + ev(nds * ldt);
+    for (int e = threadIdx.x; e < nds * nds; e += blockDim.x) {
+      const int r = e / nds, c = e - r * nds;
+      sVs[r * lds + c] = Vs[e];
+    }
     for (int e = threadIdx.x; e < ndv * ndv; e += blockDim.x) sVv[e] = Vv[e];
     for (int e = threadIdx.x; e < N; e += blockDim.x) {
       sx[e] = 0.0;
@@ -470,13 +480,13 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_ic(const FpeSolveDesc* __restr
       srhs[e] = sq[e] + rho * (sz[e] - su[e]) + sigma * sx[e];
     __syncthreads();
     // x = (Vs (x) Vv) diag(lam) (Vs (x) Vv)^T rhs
-    cta_gemm24(nds, ndv, nds, sVs, 1, nds, srhs, ndv, st1, ndv, nullptr, vec_v);  // Vs^T R
+    cta_gemm24(nds, ndv, nds, sVs, 1, lds, srhs, ndv, st1, ldt, nullptr, vec_v);  // Vs^T R
     __syncthreads();
-    cta_gemm24(nds, ndv, ndv, st1, ndv, 1, sVv, ndv, sx, ndv, slam, vec_v);  // ((Vs^T R) Vv) .* lam
+    cta_gemm24(nds, ndv, ndv, st1, ldt, 1, sVv, ndv, sx, ndv, slam, vec_v);  // ((Vs^T R) Vv) .* lam
     __syncthreads();
-    cta_gemm24(nds, ndv, nds, sVs, nds, 1, sx, ndv, st1, ndv, nullptr, vec_v);  // Vs X
+    cta_gemm24(nds, ndv, nds, sVs, lds, 1, sx, ndv, st1, ldt, nullptr, vec_v);  // Vs X
     __syncthreads();
-    cta_gemm24(nds, ndv, ndv, st1, ndv, 1, sVvT, ndv, sx, ndv, nullptr, vec_v);  // (Vs X) Vv^T
+    cta_gemm24(nds, ndv, ndv, st1, ldt, 1, sVvT, ndv, sx, ndv, nullptr, vec_v);  // (Vs X) Vv^T
     __syncthreads();
     // Config discretization: over-relaxation x^ = a x + (1 - a) z_old,
     // a = 1.6 (Boyd et al. 2011, sec. 3.4.3; the OSQP default), in the z and
