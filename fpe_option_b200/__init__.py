@@ -594,16 +594,18 @@ def interpolate_pdf(s_points, v_points, pdf, s, v) -> np.ndarray:
     ``Compute.pdf`` on ``Compute.grid_points``) interpolated at the points
     (s, v) on the GPU: Catmull-Rom bicubic, bilinear for grids with fewer than
     4 points per axis (reference src/server/interpolator.mojo:62-198)."""
-    L = _require()
-    import torch
-
     sp = np.ascontiguousarray(s_points, np.float64)
     vp = np.ascontiguousarray(v_points, np.float64)
     f = np.ascontiguousarray(pdf, np.float64)
     sq = np.ascontiguousarray(np.atleast_1d(s), np.float64)
     vq = np.ascontiguousarray(np.atleast_1d(v), np.float64)
-    if f.shape != (len(sp), len(vp)) or sq.shape != vq.shape:
+    if sp.ndim != 1 or vp.ndim != 1 or len(sp) < 2 or len(vp) < 2:
+        raise ValueError("interpolate_pdf: each grid axis needs at least 2 points")
+    if f.shape != (len(sp), len(vp)) or sq.shape != vq.shape or sq.ndim != 1:
         raise ValueError("interpolate_pdf: pdf must be len(s_points) x len(v_points), s and v of equal length")
+    L = _require()
+    import torch
+
     n = len(sq)
     if n == 0:
         return np.zeros(0)

@@ -105,3 +105,34 @@ def test_hybrid_polish_falls_back_to_fpe_jacobians(monkeypatch, sur_sign, expect
     x, info = cal.calibrate_with_surrogate(surf, _Pricer(), x0, polish="hybrid", polish_iter=10)
     assert info["polish"] == expect
     assert np.abs(x - truth).max() < 1e-6, (x, truth, info)
+
+
+def test_reference_objective_backend_carries_the_reference_settings():
+    """ReferenceObjectiveSurface prices with the objective's own settings
+    (objective.mojo:86-104: 8 x 8 knots, num_insert 251, rtol 1e-5, atol 1e-7,
+    max_step 0.02, first_step 0 = the solver's estimate, its own density sum)
+    and the calibrator's FD step 1e-6 (1 + |x|) (calibrator.mojo:64-74)."""
+    from fpe_option_b200.calibration import ReferenceObjectiveSurface
+
+    surf = Surface.grid(100.0, 0.02, [0.9, 1.0, 1.1], [0.5, 1.0])
+    be = ReferenceObjectiveSurface(surf)
+    o = be.options
+    assert be.grid == (8, 8)
+    assert (o.disc, o.precision, o.num_insert, o.complex_solve, o.radau_constants) == (0, 0, 251, 1, 1)
+    assert (o.rtol, o.atol, o.max_step, o.price_rule) == (1e-5, 1e-7, 0.02, 1)
+    assert o.first_step < 0
+    x = np.array([1.5, 0.06, 0.4, -0.5, 0.05])
+    np.testing.assert_allclose(be.steps(x), 1e-6 * (1.0 + np.abs(x)))
+    P, I = contract_tables(surf, x, be.grid)
+    assert (I[:, :2] == 8).all() and (I[:, 2] == 8).all()
+
+
+def test_interpolate_pdf_rejects_bad_shapes_before_any_device_work():
+    import fpe_option_b200 as fpe
+
+    with pytest.raises(ValueError):
+        fpe.interpolate_pdf([0.0, 1.0], [0.0, 1.0, 2.0], np.zeros((2, 2)), [0.5], [0.5])
+    with pytest.raises(ValueError):
+        fpe.interpolate_pdf([0.0], [0.0, 1.0], np.zeros((1, 2)), [0.5], [0.5])
+    with pytest.raises(ValueError):
+        fpe.interpolate_pdf([0.0, 1.0], [0.0, 1.0], np.zeros((2, 2)), [0.5, 0.7], [0.5])
