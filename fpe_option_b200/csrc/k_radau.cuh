@@ -61,6 +61,12 @@ struct KronTerm {
 struct RadauCtx {
   int ns, nv, N;
   double* work;
+  // Shared memory for the Kronecker products' intermediate: the factorization
+  // scratch, idle between factorizations and sweeps (null / 0 when the scratch
+  // lives in global memory).  An intermediate that does not fit goes to the
+  // work area.
+  double* tsm;
+  int tsm_cap;  // doubles
 };
 
 __device__ __forceinline__ double* vslot(const RadauCtx& C, int k) { return C.work + size_t(k) * C.N; }
@@ -70,7 +76,7 @@ __device__ __forceinline__ double* vslot(const RadauCtx& C, int k) { return C.wo
 __device__ void kron_apply(const RadauCtx& C, const KronTerm* terms, int nt, const double* const* X,
                            double* const* Y, int nrhs) {
   const int nv = C.nv, ns = C.ns, N = C.N;
-  double* T = vslot(C, RV_TMP);
+  double* T = (C.tsm && nt * nrhs * N <= C.tsm_cap) ? C.tsm : vslot(C, RV_TMP);
   for (int e = threadIdx.x; e < nt * nrhs * N; e += blockDim.x) {
     const int tr = e / N, idx = e - tr * N;
     const int t = tr / nrhs, r = tr - t * nrhs;
@@ -216,7 +222,8 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
     mbar_init_fence();
   }
   __syncthreads();
-  RadauCtx C{ns, nv, N, D + DL.work};
+  RadauCtx C{ns, nv, N, D + DL.work, fac_shared ? reinterpret_cast<double*>(s_fac) : nullptr,
+             fac_shared ? int(fac_need / sizeof(double)) : 0};
   const OpFactors O{ns, nv, fs, fs + ns * 7, fs + 2 * ns * 7, fs + 3 * ns * 7,
                     fv, fv + nv * 7, fv + 2 * nv * 7, fv + 3 * nv * 7, fv + 4 * nv * 7};
   FT* fbase = reinterpret_cast<FT*>(A.farena + d.off_f);
