@@ -164,3 +164,27 @@ def test_batch_struct_layouts_match_the_header(tmp_path, cname):
     out = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     assert out[0] == C.sizeof(st)
     assert out[1:] == [getattr(st, f).offset for f in fields]
+
+
+def test_batch_options_map_every_field():
+    """BatchOptions.to_c carries each Python field into the C struct (a field
+    added to the struct but not mapped would silently stay zero)."""
+    import dataclasses
+
+    import fpe_option_b200 as fpe
+    from fpe_option_b200 import _lib
+
+    c_fields = {f[0] for f in _lib.FpeBatchOptions._fields_}
+    py_fields = {f.name for f in dataclasses.fields(fpe.BatchOptions)}
+    assert c_fields == py_fields
+    vals = {}
+    for i, f in enumerate(dataclasses.fields(fpe.BatchOptions)):
+        if f.type in ("int", int):
+            vals[f.name] = 3 + i
+        elif f.type in ("bool", bool):
+            vals[f.name] = True
+        else:
+            vals[f.name] = 0.25 + i
+    o = fpe.BatchOptions(**vals).to_c()
+    for name, v in vals.items():
+        assert getattr(o, name) == (1 if v is True else v), name
