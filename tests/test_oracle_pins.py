@@ -143,3 +143,17 @@ def test_golden_fixtures(oracle):
         opt = oracle.options(**case.get("options", {}))
         p = oracle.pricer_price(**args, opt=opt)
         np.testing.assert_allclose(p, case["prices"], rtol=1e-11, atol=1e-14)
+
+
+@pytest.mark.parametrize("ns,nv,T,V0", [(24, 16, 0.6, 0.1), (32, 24, 1.2, 0.05), (40, 24, 0.3, 0.02)])
+def test_config_ic_admm_reaches_the_exact_projection(oracle, ns, nv, T, V0):
+    """The config discretization's IC ADMM (residual-balanced rho, over-
+    relaxation 1.6) converges to the nonnegative least-squares projection that
+    the exact active-set solver finds, to the ADMM's 1e-8 residual scale."""
+    h = dict(H, T=T, V0=V0)
+    kw = dict(n_s=ns, n_v=nv, option_type=8, s_max=180.0)
+    pa = oracle.Pipeline(**h, **kw, opt=oracle.options(disc=1))
+    qa = pa.array("q0")
+    qe = oracle.Pipeline(**h, **kw, opt=oracle.options(disc=1, nnls_exact=1)).array("q0")
+    assert np.linalg.norm(qa - qe) <= 1e-6 * np.linalg.norm(qe)
+    assert pa.dims()["admm"] < 500
