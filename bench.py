@@ -7,8 +7,10 @@ K/S0~U[0.8,1.2], calls/puts 50/50, grids n_s in {32,48,64} x n_v in {16,24,32}
 (sinh-stretched clamped cubic B-splines, s_max = 3 S0, v_max = 1), solved in
 one launch sequence with FP32 stage factors + FP64 Newton residuals, direct
 complex stage solve and exact Radau IIA constants.  Synthetic data (no public
-dataset is involved).  Each rank prices its own batch (seed + rank): weak
-scaling, no data-path collective.
+dataset is involved).  With N GPUs (one process each) the seeded batch has
+256 N contracts, split across the ranks by estimated solve cost; each rank
+prices its shard and one all-gather returns the whole price vector (weak
+scaling: the work per GPU stays fixed as N grows).
 
 value: prices/s with the contract descriptors resident in HBM, device time
 of the five kernels (CUDA events on the launching stream), max over ranks.
@@ -118,9 +120,14 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def rank_seed(seed: int, rank: int) -> int:
-    """Each rank prices its own batch: weak scaling, no data-path collective."""
-    return seed + rank
+def class_sample(I, per_class: int = 2):
+    """The first `per_class` contracts of each (n_s, n_v) grid class of a
+    batched-workload table, in batch order (the oracle-checked sample)."""
+    idx = []
+    for ns in (32, 48, 64):
+        for nv in (16, 24, 32):
+            idx += list(np.flatnonzero((I[:, 0] == ns) & (I[:, 1] == nv))[:per_class])
+    return np.array(sorted(idx), dtype=np.int64)
 
 
 def max_over_ranks(x: float, dist, world: int, device) -> float:
@@ -146,16 +153,20 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_baseline_run(P, I, rtol, n_threads, sample):
-    """The oracle port (single-threaded per solve, solves spread over threads)."""
+def cpu_baseline_run(P, I, rtol, n_threads, idx=None):
+    """The oracle port on the contracts idx (all when None): one solve per
+    thread, solves spread over n_threads host threads, the same discretization
+    and Radau tolerance as the GPU arm, and the reference's own complex stage
+    algorithm (GMRES(10) preconditioned by the real stage factors).  Returns
+    (prices/s, seconds, prices)."""
     from oracle import pyoracle as po
 
-    opt = po.options(disc=1, rtol=rtol, atol=rtol * 1e-2)
-    idx = np.arange(sample)
+    opt = po.options(disc=1, rtol=rtol, atol=rtol * 1e-2, radau_constants=2)
+    idx = np.arange(len(P)) if idx is None else np.asarray(idx)
     t = time.perf_counter()
-    po.price_batch(P[idx], I[idx], opt, n_threads=n_threads)
+    prices = po.price_batch(P[idx], I[idx], opt, n_threads=n_threads)
     dt = time.perf_counter() - t
-    return sample / dt, dt
+    return len(idx) / dt, dt, prices
 
 
 def run_reference_arm(args):
@@ -168,10 +179,10 @@ def run_reference_arm(args):
     sample = max(cores, min(args.cpu_sample, nc))
     rates = []
     for _ in range(args.warmup):
-        cpu_baseline_run(P, I, args.rtol, cores, min(sample, cores))
+        cpu_baseline_run(P, I, args.rtol, cores, np.arange(min(sample, cores)))
     for s in range(args.steps):
         sl = (np.arange(sample) + s * sample) % nc
-        r, _ = cpu_baseline_run(P[sl], I[sl], args.rtol, cores, sample)
+        r, _, _ = cpu_baseline_run(P, I, args.rtol, cores, sl)
         rates.append(r)
     v = float(np.mean(rates))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "prices/s",
@@ -200,7 +211,8 @@ def main():
                     help="contracts per GPU per step (smaller batches serve profiling)")
     ap.add_argument("--rtol", type=float, default=RTOL)
     ap.add_argument("--precision", type=int, default=1)
-    ap.add_argument("--cpu-sample", type=int, default=16)
+    ap.add_argument("--cpu-sample", type=int, default=18,
+                    help="CPU-baseline contracts (spread evenly over the nine grid classes)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surrogate-rate", dest="surrogate_rate", action="store_false",
                     help="skip the surrogate inference rate in the batch line")
@@ -248,8 +260,14 @@ def main():
 
     if not fpe.is_available():
         raise RuntimeError("CUDA engine unavailable")
-    nc = args.contracts
-    P, I = make_batch(nc, rank_seed(args.seed, rank))
+    from fpe_option_b200 import sharding
+
+    n_total = args.contracts * world  # weak scaling: a fixed share per GPU
+    P_all, I_all = make_batch(n_total, args.seed)
+    shards = sharding.partition(sharding.solve_costs(P_all, I_all), world)
+    mine = shards[rank]
+    P, I = P_all[mine], I_all[mine]
+    nc = len(mine)
     opts = fpe.BatchOptions(disc=1, precision=args.precision, rtol=args.rtol,
                             atol=args.rtol * 1e-2, complex_solve=2, radau_constants=2)
     arr, keep = fpe.contracts_from_arrays(P, I)
@@ -291,7 +309,9 @@ def main():
     ms = max_over_ranks(e0.elapsed_time(e1), dist, world, "cuda")
     if world > 1:
         dist.barrier()
-    value = aggregate_rate(world, nc, args.steps, ms / 1000.0)
+    value = n_total * args.steps / (ms / 1000.0)
+    # the whole batch's prices on every rank (one all-gather; untimed here)
+    p_all, st_all = sharding.gather_prices(p_out, st, shards, dist, "cuda") if world > 1 else (p_out, st)
     # ---- end to end through the public C ABI (host contracts -> host prices) -----
     pinned = torch.empty((nc, 12), dtype=torch.float64).pin_memory()
     pinned.copy_(torch.from_numpy(P))
@@ -306,25 +326,40 @@ def main():
         a2, k2 = fpe.contracts_from_arrays(Ph, I)
         pl = fpe.Plan(a2, opts, _keep=k2)
         pl.run(sptr)
-        pe, _, _, _, _ = pl.results()
+        pe, _, _, _, se = pl.results()
         pl.close()
+        if world > 1:  # every rank ends the step with the whole batch's prices
+            sharding.gather_prices(pe, se, shards, dist, "cuda")
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, world, "cuda")
-    e2e = aggregate_rate(world, nc, args.steps, e2e_s)
+    e2e = n_total * args.steps / e2e_s
     # ---- roofline of k_radau -----------------------------------------------------
     peak, peak_kind = load_peaks()
     radau_ms = ktimes[3]
     achieved = stats["factor_bytes"] / (radau_ms / 1000.0) / 1e9
     traffic = load_traffic()
     # ---- CPU baseline (oracle port), rank 0, bounded sample -------------------------
+    # The sample is two contracts of each of the nine grid classes; its oracle
+    # prices also give this run's error against the FP64 oracle.
     cpu = None
+    oracle_err = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        sample = max(min(cores, nc), min(args.cpu_sample, nc))
-        rate, dt = cpu_baseline_run(P, I, args.rtol, cores, sample)
+        sidx = class_sample(I, max(1, args.cpu_sample // 9))
+        rate, dt, p_orc = cpu_baseline_run(P, I, args.rtol, cores, sidx)
         cpu = {"value": rate, "unit": "prices/s", "cores": cores, "kind": "port",
-               "sample": f"first {sample} contracts of the same batch, oracle C++ FP64 "
-                         f"restatement on {cores} host threads, {dt:.1f} s"}
+               "sample": f"{len(sidx)} contracts of the same batch ({len(sidx) // 9} per grid class), oracle C++ "
+                         f"FP64 restatement on {cores} host threads, {dt:.1f} s"}
+        e_orc = np.abs(p_out[sidx] - p_orc) / np.maximum(np.abs(p_orc), floor)
+        p64, _ = fpe.price_batch(P[sidx], I[sidx], fpe.BatchOptions(
+            disc=1, precision=0, rtol=args.rtol, atol=args.rtol * 1e-2, complex_solve=2, radau_constants=2))
+        e64 = np.abs(p64 - p_orc) / np.maximum(np.abs(p_orc), floor)
+        oracle_err = {"max_rel_err_vs_oracle": float(e_orc.max()), "median_rel_err_vs_oracle": float(np.median(e_orc)),
+                      "contracts": int(len(sidx)), "err_floor": floor,
+                      "fp64_max_rel_err_vs_oracle": float(e64.max()),
+                      "note": "this run's mixed-precision prices against the oracle's FP64 prices at the same rtol, "
+                              "on the CPU-baseline sample (every grid class); fp64_...: the GPU's FP64-factor "
+                              "path on the same sample and rtol"}
     # ---- surrogate inference rate (3-member BF16 tensor-core ensemble) ---------------
     sur = None
     if rank == 0 and world == 1 and args.surrogate_rate:
@@ -419,6 +454,7 @@ def main():
                        "l2": "inputs and factors larger than L2 (126 MB)",
                        "max_rel_err_vs_fp64": float(rel.max()), "err_floor": floor,
                        "max_rel_err_unfloored": float(rel_unfloored.max()),
+                       "oracle_parity": oracle_err,
                        "fp64_reference_rtol": REF_RTOL,
                        "status_ok": bool((st == 0).all() and (st_ref == 0).all())},
             "e2e": {"value": e2e, "unit": "prices/s", "h2d_bytes_per_step": int(h2d),

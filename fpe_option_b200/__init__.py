@@ -447,6 +447,9 @@ class BatchOptions:
     max_step: float = 0.0    # <= 0: T/5 (the reference Pricer); > 0: absolute cap
     first_step: float = 0.0  # 0: 1e-6 (Pricer); < 0: the Radau solver's own estimate
     price_rule: int = 0      # 1: the calibration objective's undiscounted sum (reference disc)
+    max_steps: int = 0       # <= 0: 100000 accepted steps (the reference cap)
+    fp64_retry: int = 0      # precision 1: re-solve failed solves with FP64 factors (0/1 on, < 0 off)
+    stage_wait_cycles: int = 0  # <= 0: ~1 s bounded wait per staged sweep stage
 
     def to_c(self) -> _lib.FpeBatchOptions:
         o = _lib.FpeBatchOptions()
@@ -459,6 +462,8 @@ class BatchOptions:
         o.complex_solve = self.complex_solve
         o.radau_constants = self.radau_constants
         o.max_step, o.first_step, o.price_rule = self.max_step, self.first_step, self.price_rule
+        o.max_steps, o.fp64_retry = self.max_steps, self.fp64_retry
+        o.stage_wait_cycles = self.stage_wait_cycles
         return o
 
 
@@ -522,6 +527,19 @@ class Plan:
                 "factor_bytes", "worst_status", "kcyc_factor", "kcyc_solve", "kcyc_kron",
                 "kcyc_total", "kcyc_factor_gj", "kcyc_factor_gemm"]
         return dict(zip(keys, list(out)))
+
+    def retried(self) -> int:
+        """Solves of the last ``results()`` re-solved with FP64 factors after a
+        mixed-precision failure."""
+        return int(self._L.fpe_plan_retried(self._h))
+
+    def solve_info(self) -> np.ndarray:
+        """Per-solve counters of the last run, (n_solves, 32) int32 in the plan's
+        solve order (see fpe_plan_solve_info in include/fpe_engine.h)."""
+        out = np.zeros((self.n_solves, 32), np.int32)
+        if self._L.fpe_plan_solve_info(self._h, out.ctypes.data_as(_lib.ip)) < 0:
+            raise RuntimeError("fpe_plan_solve_info failed")
+        return out
 
     def kernel_times(self, stream: int | None = None) -> list[float]:
         """Run once with CUDA events around each kernel; returns ms for

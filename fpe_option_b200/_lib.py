@@ -55,7 +55,8 @@ class FpeBatchOptions(C.Structure):
                 ("rtol", d), ("atol", d), ("ic_sigma_s", d), ("ic_sigma_v", d), ("ic_sub", i32),
                 ("greeks", i32), ("rel_s", d), ("rel_v", d), ("complex_solve", i32),
                 ("radau_constants", i32), ("max_step", d), ("first_step", d),
-                ("price_rule", i32)]
+                ("price_rule", i32), ("max_steps", i32), ("fp64_retry", i32),
+                ("stage_wait_cycles", i64)]
 
 
 # Every symbol declared in include/*.h.
@@ -67,7 +68,7 @@ EXPORTED = [
     "fpe_compute_free_oneshot", "fpe_plan_create", "fpe_plan_run", "fpe_plan_results",
     "fpe_plan_stats", "fpe_plan_sizes", "fpe_plan_destroy", "fpe_price_batch",
     "fpe_compute_create_ex", "fpe_compute_basis_csr", "fpe_device_available",
-    "fpe_plan_kernel_times", "fpe_price_noalloc", "fpe_heston_cf_batch", "fpe_heston_cf_price",
+    "fpe_plan_kernel_times", "fpe_plan_retried", "fpe_plan_solve_info", "fpe_price_noalloc", "fpe_heston_cf_batch", "fpe_heston_cf_price",
     "fpe_pdf_interpolate",
     # include/fpe_surrogate.h
     "fpe_mlp_create", "fpe_mlp_destroy", "fpe_mlp_layout", "fpe_mlp_get_params",
@@ -122,6 +123,10 @@ def load():
     L.fpe_plan_kernel_times.argtypes = [cp, vp, C.POINTER(C.c_float)]
     L.fpe_plan_sizes.restype = i32
     L.fpe_plan_sizes.argtypes = [cp, ip, ip]
+    L.fpe_plan_retried.restype = i32
+    L.fpe_plan_retried.argtypes = [cp]
+    L.fpe_plan_solve_info.restype = i32
+    L.fpe_plan_solve_info.argtypes = [cp, ip]
     L.fpe_plan_destroy.argtypes = [cp]
     L.fpe_price_batch.restype = i32
     L.fpe_price_batch.argtypes = [C.POINTER(FpeContract), i32, C.POINTER(FpeBatchOptions),

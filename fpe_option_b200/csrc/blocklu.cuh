@@ -615,7 +615,7 @@ __device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int n
 // fpe_fac_scratch_elems(nv) elements each.
 template <typename FT>
 __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC, FT* scr_r,
-                                Cx<FT>* scr_c, long long (&tcyc)[2]) {
+                                Cx<FT>* scr_c, long long (&tcyc)[3]) {
   const int ns = LR.ns;
   FacScratch<FT> SR;
   SR.init(scr_r, LR.nv);
@@ -679,6 +679,8 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
           fac_update<FT, false>(LR, SR, i, nr, 1, nr * nr, lt, nt);
           if (LC) fac_update<Cx<FT>, false>(*LC, SC, i, nr, 1, nr * nr, lt, nt);
         }
+        // this warp's own time in the overlapped phase, before the barrier
+        tcyc[2] += clock64() - t3;
       } else {
         fac_update<FT, false>(LR, SR, i, nr, 1, nr * nr, threadIdx.x, blockDim.x);
         if (LC) fac_update<Cx<FT>, false>(*LC, SC, i, nr, 1, nr * nr, threadIdx.x, blockDim.x);
@@ -846,9 +848,10 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
 // Staged fused block solve.
 //
 // The 2 ns + 1 block rows of a solve (forward rows 0..ns, backward rows
-// ns-1..0) stream through two shared-memory stage buffers by bulk copies:
-// while the CTA multiplies stage s, stage s + 1 is in flight, and thread 0
-// issues stage s + 2 into the freed buffer after the row's barrier.  A stage
+// ns-1..0) stream through nbuf (2 to 4) shared-memory stage buffers by bulk
+// copies: while the CTA multiplies stage s, stages s + 1 .. s + nbuf - 1 are
+// in flight, and one thread issues stage s + nbuf into the freed buffer after
+// the row's barrier, so each copy has nbuf - 1 stage times to land.  A stage
 // holds the blocks the row needs from each factor (forward row i: L_{i,i-3+g},
 // g < 3, and P^-1_{i-1}; backward row i: W_{i,i+1+g}), one slot per block with
 // a 64-byte gap so that the slots of a complex row group start in alternate
@@ -857,23 +860,31 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
 // One thread owns one row of a real system; Gc lanes own one row of the
 // complex system and split its blocks.
 // --------------------------------------------------------------------------
+constexpr int kMaxStageBufs = 4;
+
 struct SolveStage {
-  unsigned char* buf[2];     // stage buffers (shared, 16-byte aligned)
+  unsigned char* buf[kMaxStageBufs];  // stage buffers (shared, 16-byte aligned)
+  int nbuf;                  // buffers in use (2 .. kMaxStageBufs)
   void* ring;                // 4 segments x nv per right-hand-side array (nr real, re, im), of the
                              // sweep's accumulation type (float with FP32 factors, else double)
-  unsigned long long* bar;   // 2 mbarriers (shared)
+  unsigned long long* bar;   // nbuf mbarriers (shared)
   int* err;                  // shared flag: a bounded wait gave up
   int slot_r, slot_c;        // bytes per staged real / complex block slot
+  long long wait_limit;      // SM cycles a stage waits for its copies
+  long long* wait_cycles;    // accumulates this thread's cycles spent in those waits
 };
 
 __host__ __device__ __forceinline__ int stage_slot_bytes(int nv, int esz) {
   return fpe_block_stride(nv) * esz + 64;
 }
-// Bytes of the two stage buffers plus the ring for block size nv, element size
-// esz of the real factor, with or without the complex factor.
-__host__ __device__ __forceinline__ int stage_total_bytes(int nv, int esz, bool cplx) {
-  const int stage = 4 * stage_slot_bytes(nv, esz) + (cplx ? 4 * stage_slot_bytes(nv, 2 * esz) : 0);
-  return 2 * stage + 4 * nv * 4 * 8;
+// Bytes of one stage buffer for block size nv, element size esz of the real
+// factor, with or without the complex factor.
+__host__ __device__ __forceinline__ int stage_bytes(int nv, int esz, bool cplx) {
+  return 4 * stage_slot_bytes(nv, esz) + (cplx ? 4 * stage_slot_bytes(nv, 2 * esz) : 0);
+}
+// Bytes of nbuf stage buffers plus the ring.
+__host__ __device__ __forceinline__ int stage_total_bytes(int nv, int esz, bool cplx, int nbuf = 2) {
+  return nbuf * stage_bytes(nv, esz, cplx) + 4 * nv * 4 * 8;
 }
 
 // Block (row, kk) of stage s and slot g; nullptr when the row has no such block.
@@ -893,9 +904,9 @@ __device__ __forceinline__ const ET* stage_block(const BlockLU<ET>& L, int s, in
 // generic-proxy writes (the factorization) before the async-proxy reads; the
 // factor does not change during a sweep, so only a sweep's first issue needs it.
 template <typename FT>
-__device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s, bool gfence) {
-  unsigned long long* bar = P.bar + (s & 1);
-  unsigned char* dst = P.buf[s & 1];
+__device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s, int b, bool gfence) {
+  unsigned long long* bar = P.bar + b;
+  unsigned char* dst = P.buf[b];
   const int nv = S.R ? S.R->nv : S.Cf->nv;
   const uint32_t br = uint32_t(fpe_block_stride(nv)) * sizeof(FT);
   const uint32_t bc = 2 * br;
@@ -1001,8 +1012,10 @@ __device__ __forceinline__ void col_dot_c(const Cx<T>* col, const double* xr, co
 }
 
 // Returns false when a bounded wait gave up (the solve result is then invalid
-// and *P.err is set).  `phase` holds the parity bits of the two barriers and
-// is carried across calls; every thread of the CTA calls this.
+// and *P.err is set).  `phase` holds the parity bits of the nbuf barriers and
+// is carried across calls (a sweep leaves every barrier with an even number
+// of completed phases or not: each thread tracks them); every thread of the
+// CTA calls this.
 template <typename FT>
 __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uint32_t& phase) {
   if (*P.err) return false;
@@ -1029,19 +1042,21 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
 
   // the thread that issues the copies: an idle one when the roles leave one
   const int issuer = (int(blockDim.x) - 1 >= max(nreal, cbase + (S.nc > 0 ? Gc * nv : 0))) ? int(blockDim.x) - 1 : 0;
+  const int nb = P.nbuf;
   uint32_t pend = 0;  // buffers with a stage in flight (the issuer's view)
   if (tid == issuer) {
-    stage_issue<FT>(S, P, 0, true);
-    pend |= 1u;
-    if (nstage > 1) {
-      stage_issue<FT>(S, P, 1, false);
-      pend |= 2u;
+    for (int q = 0; q < nb && q < nstage; ++q) {
+      stage_issue<FT>(S, P, q, q, q == 0);
+      pend |= 1u << q;
     }
   }
   bool ok = true;
-  for (int s = 0; s < nstage; ++s) {
-    const int b = s & 1;
-    if (mbar_wait_bounded(P.bar + b, (phase >> b) & 1u, kBulkWaitLimit)) {
+  int b = 0;  // buffer of stage s: s mod nb
+  for (int s = 0; s < nstage; ++s, b = (b + 1 == nb) ? 0 : b + 1) {
+    const long long tw0 = clock64();
+    const bool landed = mbar_wait_bounded(P.bar + b, (phase >> b) & 1u, P.wait_limit);
+    *P.wait_cycles += clock64() - tw0;
+    if (landed) {
       phase ^= 1u << b;
       pend &= ~(1u << b);
     } else {
@@ -1124,15 +1139,16 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
       ok = false;
       break;
     }
-    if (tid == issuer && s + 2 < nstage) {
-      stage_issue<FT>(S, P, s + 2, false);
+    if (tid == issuer && s + nb < nstage) {
+      stage_issue<FT>(S, P, s + nb, b, false);
       pend |= 1u << b;
     }
   }
   if (!ok && tid == issuer) {
-    // let copies still in flight land (bounded) before the buffers are reused
-    for (int b = 0; b < 2; ++b)
-      if ((pend >> b) & 1u) mbar_wait_bounded(P.bar + b, (phase >> b) & 1u, kBulkWaitLimit);
+    // let copies still in flight land before the buffers are reused: the full
+    // (about one second) limit, whatever the stage waits were given
+    for (int q = 0; q < nb; ++q)
+      if ((pend >> q) & 1u) mbar_wait_bounded(P.bar + q, (phase >> q) & 1u, kBulkWaitLimit);
   }
   __syncthreads();
   return ok;

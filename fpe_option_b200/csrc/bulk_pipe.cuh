@@ -64,10 +64,35 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t 
   return ok != 0;
 }
 
+// Non-blocking test of the phase (never suspends the thread).
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n"
+      "  .reg .pred p;\n"
+      "  mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "  selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Limits below this many cycles poll with test_wait: try_wait may suspend the
+// thread for a system-dependent time, longer than such a limit.
+constexpr long long kShortWaitCycles = 1LL << 20;
+
 // Wait for the phase of `bar` with the given parity to complete; gives up
 // after `limit` SM clock cycles and returns false.
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, uint32_t parity, long long limit) {
   const long long t0 = clock64();
+  if (limit < kShortWaitCycles) {
+    while (!mbar_test_wait(bar, parity)) {
+      if (clock64() - t0 > limit) return false;
+    }
+    return true;
+  }
   while (!mbar_try_wait(bar, parity)) {
     if (clock64() - t0 > limit) return false;
   }

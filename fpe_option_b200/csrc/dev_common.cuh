@@ -57,7 +57,7 @@ __device__ __forceinline__ double block_max1(double v, double* red) {
 
 // Block-wide bitonic sort of n doubles in shared memory (buf holds a power of
 // two >= n entries; the tail is padded with +inf).
-__device__ void block_sort(double* buf, int n, int cap_pow2) {
+static __device__ void block_sort(double* buf, int n, int cap_pow2) {
   for (int i = n + threadIdx.x; i < cap_pow2; i += blockDim.x) buf[i] = CUDART_INF;
   __syncthreads();
   for (int k = 2; k <= cap_pow2; k <<= 1) {
@@ -89,7 +89,7 @@ __device__ __forceinline__ double bs_base(const double* t, int nt, double x, int
   return 0.0;
 }
 
-__device__ double bs_value(const double* t, int nt, double x, int i, int deg) {
+static __device__ double bs_value(const double* t, int nt, double x, int i, int deg) {
   int nb = nt - deg - 1;
   if (i < 0 || i >= nb) return 0.0;
   double work[4];
@@ -109,7 +109,7 @@ __device__ double bs_value(const double* t, int nt, double x, int i, int deg) {
 }
 
 // basis.mojo:122-213 (cubic derivative via degree-2 splines).
-__device__ double bs_deriv3(const double* t, int nt, double x, int col) {
+static __device__ double bs_deriv3(const double* t, int nt, double x, int col) {
   double left = 0.0, right = 0.0;
   double d1 = t[col + 3] - t[col];
   if (d1 != 0.0) left = 3.0 / d1 * bs_value(t, nt, x, col, 2);
@@ -123,7 +123,7 @@ __device__ double bs_deriv3(const double* t, int nt, double x, int col) {
 // Neumann end merges B_0 (left) / B_{nb-1} (right) into the adjacent dof, a
 // Dirichlet end drops it.  Values with |v| <= 1e-12 are dropped as in
 // basis.mojo:85 / :160 before recombination.
-__device__ void recombined_window(const double* t, int nt, double x, bool lneu, bool rneu,
+static __device__ void recombined_window(const double* t, int nt, double x, bool lneu, bool rneu,
                                   int* c0_out, double* B, double* dB) {
   const int nb = nt - 4;
   const int rc = nb - 2;

@@ -25,8 +25,16 @@
 #include "k_ic.cuh"
 #include "k_interp.cuh"
 #include "k_payoff.cuh"
-#include "k_radau.cuh"
+#include "radau_launch.h"
 #include "k_setup.cuh"
+
+static_assert(FPE_SOLVE_INFO_WORDS == FPE_INFO_COUNT, "per-solve info words of the C ABI");
+
+// Stage buffers of the staged sweeps (2 .. 4; a solve uses as many as its
+// shared scratch holds, up to this).
+#ifndef FPE_SWEEP_BUFS
+#define FPE_SWEEP_BUFS 2
+#endif
 
 namespace {
 
@@ -66,8 +74,8 @@ Context& ctx() {
     if (cudaFuncSetAttribute(fpe::k_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess) return;
     const int ic_lim = lim - int(sizeof(fpe::IcSmem)) - 1024;
     if (cudaFuncSetAttribute(fpe::k_ic, cudaFuncAttributeMaxDynamicSharedMemorySize, ic_lim) != cudaSuccess) return;
-    if (cudaFuncSetAttribute(fpe::k_radau<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess) return;
-    if (cudaFuncSetAttribute(fpe::k_radau<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) != cudaSuccess) return;
+    if (fpe::radau_allow_smem<double>(lim) != cudaSuccess) return;
+    if (fpe::radau_allow_smem<float>(lim) != cudaSuccess) return;
     c.ok = true;
   });
   return c;
@@ -86,12 +94,15 @@ struct Pricing {  // one Pricer.price call: contract (possibly bumped)
 
 // option_types.mojo:13-32 + heston_params.mojo:19-33
 bool pricing_valid(const Pricing& p, const double* K) {
+  // every parameter finite (NaN and Inf fail here, not inside a solve)
+  for (double x : {p.kappa, p.theta, p.sigma, p.rho, p.r, p.T, p.S0, p.V0, p.barrier, p.smin, p.smax})
+    if (!std::isfinite(x)) return false;
   if (!(p.kappa > 0 && p.theta > 0 && p.sigma > 0 && p.T > 0 && p.S0 > 0 && p.V0 >= 0 &&
         p.smin >= 0 && p.smax > p.smin && p.rho >= -1 && p.rho <= 1))
     return false;
   if (p.type < 0 || p.type > 9 || p.n_strikes <= 0) return false;
   for (int i = 0; i < p.n_strikes; ++i)
-    if (!(K[i] > 0.0)) return false;
+    if (!(K[i] > 0.0) || !std::isfinite(K[i])) return false;
   if (p.type <= 3) {
     if (p.barrier <= 0.0 || p.barrier >= p.S0) return false;
   } else if (p.type <= 7) {
@@ -110,6 +121,9 @@ struct Opts {
          rel_v = 0.1;
   double max_step = 0.0, first_step = 0.0;  // 0: the reference Pricer's T/5 and 1e-6
   int price_rule = 0;                       // 1: calibration-objective integration
+  int max_steps = 0;                        // <= 0: 100000 (radau.mojo:257-263)
+  int fp64_retry = 1;                       // re-solve failed mixed solves with FP64 factors
+  long long stage_wait = 0;                 // <= 0: about one second
 };
 
 Opts opts_from(const FpeBatchOptions* o, int default_num_insert) {
@@ -137,6 +151,9 @@ Opts opts_from(const FpeBatchOptions* o, int default_num_insert) {
   if (o->max_step > 0) r.max_step = o->max_step;
   r.first_step = std::isfinite(o->first_step) ? o->first_step : 0.0;
   r.price_rule = (o->price_rule == 1 && o->disc == 0) ? 1 : 0;
+  r.max_steps = o->max_steps > 0 ? o->max_steps : 0;
+  r.fp64_retry = o->fp64_retry < 0 ? 0 : 1;
+  r.stage_wait = o->stage_wait_cycles > 0 ? (long long)o->stage_wait_cycles : 0;
   return r;
 }
 
@@ -165,6 +182,8 @@ FpeSolveDesc make_desc(const Pricing& p, int solve_type, double barrier, const O
   d.barrier = barrier;
   d.rtol = o.rtol; d.atol = o.atol;
   d.max_step = o.max_step; d.first_step = o.first_step;
+  d.max_steps = o.max_steps;
+  d.stage_wait = o.stage_wait;
   d.price_rule = o.price_rule;
   d.ic_sigma_s = o.ic_sigma_s; d.ic_sigma_v = o.ic_sigma_v;
   d.type = solve_type;
@@ -235,6 +254,8 @@ struct FpePlan {
   std::vector<double> h_prices;
   std::vector<int32_t> h_infos;
   bool ran = false, fetched = false;
+  bool retry_pending = false;  // results not yet checked for FP64 re-solves
+  int n_retried = 0;
   cudaStream_t stream = nullptr;
 };
 
@@ -330,13 +351,13 @@ static int plan_launch(FpePlan* P, cudaStream_t s, int from, int to) {
     if (P->o.precision == 0) {
       fpe::RadauKernelArgs<double> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena,
                                      P->d_traj, 0, P->o.complex_mode, P->fac_global,
-                                     rk.u1, rk.alph, rk.beta, rk.ti13, P->radau_smem};
-      fpe::k_radau<double><<<grid, block, P->radau_smem, s>>>(a);
+                                     rk.u1, rk.alph, rk.beta, rk.ti13, P->radau_smem, FPE_SWEEP_BUFS};
+      CK(fpe::launch_radau<double>(a, grid, dim3(FPE_RADAU_THREADS), P->radau_smem, s));
     } else {
       fpe::RadauKernelArgs<float> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena,
                                     P->d_traj, P->o.refine, P->o.complex_mode, P->fac_global,
-                                    rk.u1, rk.alph, rk.beta, rk.ti13, P->radau_smem};
-      fpe::k_radau<float><<<grid, block, P->radau_smem, s>>>(a);
+                                    rk.u1, rk.alph, rk.beta, rk.ti13, P->radau_smem, FPE_SWEEP_BUFS};
+      CK(fpe::launch_radau<float>(a, grid, dim3(FPE_RADAU_THREADS), P->radau_smem, s));
     }
     ++launches;
   }
@@ -548,6 +569,50 @@ static int plan_combine(FpePlan* P, double* prices, double* delta, double* gamma
   return worst;
 }
 
+// A mixed-precision solve that ends with a solver failure (a singular or
+// non-finite FP32 factor, the step caps, a sweep's wait that gave up) is
+// solved again with FP64 factors: the failed solves' descriptors form one
+// sub-plan that runs all five phases, and its prices and status words replace
+// the first attempt's.  Returns the number of re-solved solves, < 0 on error.
+static bool solver_failure(int st) { return st >= FPE_ERR_SINGULAR && st <= FPE_ERR_TIMEOUT; }
+
+static int plan_retry_fp64(FpePlan* P) {
+  if (P->o.precision == 0 || !P->o.fp64_retry) return 0;
+  std::vector<int> first, fail;
+  price_slots(P, first);
+  for (size_t s = 0; s < P->descs.size(); ++s)
+    if (solver_failure(P->h_infos[s * FPE_INFO_COUNT + FPE_INFO_STATUS])) fail.push_back(int(s));
+  if (fail.empty()) return 0;
+  auto* R = new FpePlan();
+  R->o = P->o;
+  R->o.precision = 0;
+  int slot = 0;
+  for (int s : fail) {
+    FpeSolveDesc d = P->descs[s];
+    d.stage_wait = 0;  // the default bounded wait
+    d.strike_off = slot;
+    for (int j = 0; j < d.n_strikes; ++j) R->strikes.push_back(P->strikes[first[s] + j]);
+    slot += d.n_strikes;
+    R->descs.push_back(d);
+  }
+  R->n_price_slots = slot;
+  plan_layout(R, 8);
+  int rc = plan_upload(R);
+  if (rc == 0 && plan_launch(R, R->stream, 0, 5) < 0) rc = -1;
+  if (rc == 0 && plan_fetch(R) < 0) rc = -1;
+  if (rc == 0) {
+    for (size_t k = 0; k < fail.size(); ++k) {
+      const int s = fail[k];
+      for (int j = 0; j < P->descs[s].n_strikes; ++j)
+        P->h_prices[first[s] + j] = R->h_prices[R->descs[k].strike_off + j];
+      std::memcpy(&P->h_infos[size_t(s) * FPE_INFO_COUNT], &R->h_infos[k * FPE_INFO_COUNT],
+                  FPE_INFO_COUNT * sizeof(int32_t));
+    }
+  }
+  plan_free(R);
+  return rc < 0 ? -1 : int(fail.size());
+}
+
 // --------------------------------------------------------------------------
 // Stepwise pipeline (reference src/server/compute_pipeline.mojo:17-171)
 // --------------------------------------------------------------------------
@@ -655,6 +720,7 @@ static int price_fresh(const FpeContract& k, const Opts& o, const double* K, int
   int rc = plan_upload(P);
   if (rc == 0 && plan_launch(P, P->stream, 0, 5) < 0) rc = -1;
   if (rc == 0 && plan_fetch(P) < 0) rc = -1;
+  if (rc == 0 && plan_retry_fp64(P) < 0) rc = -1;
   std::vector<int32_t> st(nK);
   if (rc == 0) plan_combine(P, out, d, g, v, st.data());
   plan_free(P);
@@ -726,6 +792,7 @@ int32_t fpe_plan_run(FpePlan* P, void* stream) {
     cudaEventDestroy(ev);
   }
   P->fetched = false;
+  P->retry_pending = true;
   int n = plan_launch(P, s, 0, 5);
   if (n < 0) return -1;
   if (s != P->stream) {
@@ -743,7 +810,21 @@ int32_t fpe_plan_results(FpePlan* P, double* prices, double* delta, double* gamm
                          int32_t* status) {
   if (!P || !P->ran) return -1;
   if (plan_fetch(P) < 0) return -1;
+  if (P->retry_pending) {
+    P->retry_pending = false;
+    P->n_retried = plan_retry_fp64(P);
+    if (P->n_retried < 0) return -1;
+  }
   return plan_combine(P, prices, delta, gamma, vega, status);
+}
+
+int32_t fpe_plan_retried(FpePlan* P) { return P ? P->n_retried : -1; }
+
+int32_t fpe_plan_solve_info(FpePlan* P, int32_t* out) {
+  if (!P || !out) return -1;
+  if (plan_fetch(P) < 0) return -1;
+  std::memcpy(out, P->h_infos.data(), P->h_infos.size() * sizeof(int32_t));
+  return int32_t(P->descs.size());
 }
 
 int32_t fpe_plan_stats(FpePlan* P, int64_t* out) {
@@ -792,6 +873,7 @@ int32_t fpe_plan_kernel_times(FpePlan* P, void* stream, float* ms) {
     CK(cudaStreamWaitEvent(s, ev[0], 0));
   }
   P->fetched = false;
+  P->retry_pending = true;
   for (int k = 0; k < 5; ++k) {
     CK(cudaEventRecord(ev[k], s));
     if (plan_launch(P, s, k, k + 1) < 0) return -1;
@@ -1053,46 +1135,59 @@ void fpe_compute_free_oneshot(FpeOneshotResult* r) {
 // ==========================================================================
 // Allocation-free pricing of one contract.
 //
-// Some callers cannot allocate device memory at pricing time: code that runs
-// while a CUDA stream is being captured into a graph (allocation calls there
-// either fail or get frozen into the graph), real-time and embedded hosts whose
-// GPU memory budget is fixed at start-up, and plug-ins living inside another
-// application that owns the device memory pool.  fpe_price_noalloc serves them
-// from one file-scope static device array instead of per-call allocations; the
-// caller passes the contract and receives the prices.
+// Some callers cannot allocate device memory at pricing time: real-time and
+// embedded hosts whose GPU memory budget is fixed at start-up, and plug-ins
+// living inside another application that owns the device memory pool (its
+// allocator may be exhausted or forbidden to them).  fpe_price_noalloc serves
+// them from one file-scope static device array instead of per-call
+// allocations; the caller passes the contract and receives the prices.
 //
 // The array (FPE_NOALLOC_SCRATCH_BYTES, 64 MiB) is held by every GPU that loads
-// this library until the process exits.  Its device address is obtained with
-// cudaGetSymbolAddress once per device, on that device's first call (so make
-// the first call on each device before any stream capture).  Every call shares
-// the array and it keeps the previous call's contents: the per-solve status
-// words and the price slots are cleared at the start of each call, everything
-// else is fully rewritten by the kernels.  Calls that overlap on the GPU (the
-// same device, different streams or threads without ordering) race on the
-// array and must be serialized by the caller.
+// this library until the process exits.  Each device is set up on its first
+// call, with that device current: the array's device address
+// (cudaGetSymbolAddress), a stream of its own and the kernels' shared-memory
+// opt-in.  Every call shares the array and it keeps the previous call's
+// contents: the per-solve status words and the price slots are cleared at the
+// start of each call, everything else is fully rewritten by the kernels.  Calls
+// that overlap on the GPU (the same device, different streams or threads
+// without ordering) race on the array and must be serialized by the caller.
+// The call copies its results to host memory and waits for its stream, so it
+// cannot run on a stream that is being captured into a graph: it checks that
+// first and returns FPE_NOALLOC_ERR_CAPTURE without enqueuing anything.
 // ==========================================================================
 #define FPE_NOALLOC_SCRATCH_BYTES (64ull << 20)
 #define FPE_NOALLOC_MAX_DEVICES 64
 static __device__ __align__(256) unsigned char g_fpe_noalloc_scratch[FPE_NOALLOC_SCRATCH_BYTES];
 
-static unsigned char* noalloc_base(int device, int* err) {
-  static unsigned char* base[FPE_NOALLOC_MAX_DEVICES] = {nullptr};
+struct NoallocDevice {
+  unsigned char* base = nullptr;  // device address of the static array
+  cudaStream_t stream = nullptr;  // used when the caller passes no stream
+  int smem_optin = 0;
+};
+
+// Per-device set-up on the device's first call (the current device).
+static NoallocDevice* noalloc_device(int device) {
+  static NoallocDevice devs[FPE_NOALLOC_MAX_DEVICES];
   static std::mutex mu;
-  if (device < 0 || device >= FPE_NOALLOC_MAX_DEVICES) {
-    *err = -1;
-    return nullptr;
-  }
+  if (device < 0 || device >= FPE_NOALLOC_MAX_DEVICES) return nullptr;
   std::lock_guard<std::mutex> lock(mu);
-  if (!base[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_fpe_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      *err = -1;
-      return nullptr;
-    }
-    base[device] = static_cast<unsigned char*>(p);
-  }
-  return base[device];
+  NoallocDevice& D = devs[device];
+  if (D.base) return &D;
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_fpe_noalloc_scratch) != cudaSuccess || !p) return nullptr;
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) return nullptr;
+  if (cudaFuncSetAttribute(fpe::k_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess ||
+      cudaFuncSetAttribute(fpe::k_ic, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           optin - int(sizeof(fpe::IcSmem)) - 1024) != cudaSuccess ||
+      fpe::radau_allow_smem<double>(optin) != cudaSuccess || fpe::radau_allow_smem<float>(optin) != cudaSuccess)
+    return nullptr;
+  cudaStream_t st = nullptr;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  D.stream = st;
+  D.smem_optin = optin;
+  D.base = static_cast<unsigned char*>(p);
+  return &D;
 }
 
 extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatchOptions* opt,
@@ -1101,14 +1196,17 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
   const int nk = contract->n_strikes;
   if (nk <= 0 || nk > FPE_MAX_STRIKES || !contract->strikes) return FPE_NOALLOC_ERR_SIZE;
   if (opt && opt->greeks) return -1;
-  Context& C = ctx();
-  if (!C.ok) return -1;
+  if (cuda_stream) {  // a capturing stream would be invalidated by the host copies and the wait
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(static_cast<cudaStream_t>(cuda_stream), &cs) != cudaSuccess) return -1;
+    if (cs != cudaStreamCaptureStatusNone) return FPE_NOALLOC_ERR_CAPTURE;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -1;
-  int err = 0;
-  unsigned char* base = noalloc_base(dev, &err);
-  if (!base) return -1;
-  cudaStream_t s = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : C.stream;
+  NoallocDevice* ND = noalloc_device(dev);
+  if (!ND) return -1;
+  unsigned char* base = ND->base;
+  cudaStream_t s = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ND->stream;
   const Opts o = opts_from(opt, 50);
 
   // Pricing and its one or two device solves (in-out parity for knock-ins).
@@ -1188,7 +1286,7 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
     }
     return FPE_NOALLOC_ERR_SIZE;  // the contract's grids need more than the static array
   }
-  const size_t optin = size_t(C.smem_optin > 0 ? C.smem_optin : 232448);
+  const size_t optin = size_t(ND->smem_optin);
   const int fac_global = smem_max > optin ? 1 : 0;
   const size_t radau_smem = fac_global ? smem_base : smem_max;
   const size_t ic_smem = ic <= optin - sizeof(fpe::IcSmem) - 1024 ? ic : 0;
@@ -1212,12 +1310,12 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
   const fpe::RadauConstants rk = fpe::radau_constants(o.radau_exact != 0);
   if (o.precision == 0) {
     fpe::RadauKernelArgs<double> a{g_desc, g_d, g_i, g_info, g_f, nullptr, 0, o.complex_mode,
-                                   fac_global, rk.u1, rk.alph, rk.beta, rk.ti13, radau_smem};
-    fpe::k_radau<double><<<grid, block, radau_smem, s>>>(a);
+                                   fac_global, rk.u1, rk.alph, rk.beta, rk.ti13, radau_smem, FPE_SWEEP_BUFS};
+    CK(fpe::launch_radau<double>(a, grid, dim3(FPE_RADAU_THREADS), radau_smem, s));
   } else {
     fpe::RadauKernelArgs<float> a{g_desc, g_d, g_i, g_info, g_f, nullptr, o.refine, o.complex_mode,
-                                  fac_global, rk.u1, rk.alph, rk.beta, rk.ti13, radau_smem};
-    fpe::k_radau<float><<<grid, block, radau_smem, s>>>(a);
+                                  fac_global, rk.u1, rk.alph, rk.beta, rk.ti13, radau_smem, FPE_SWEEP_BUFS};
+    CK(fpe::launch_radau<float>(a, grid, dim3(FPE_RADAU_THREADS), radau_smem, s));
   }
   fpe::k_payoff<<<grid, block, 0, s>>>(g_desc, g_d, g_i, g_info, g_k, g_p);
   CK(cudaGetLastError());

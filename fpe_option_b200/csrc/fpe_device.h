@@ -7,6 +7,10 @@
 #include <stdint.h>
 
 #define FPE_BLOCK 256
+// Threads of the persistent Radau kernel's CTA (one CTA per solve).
+#ifndef FPE_RADAU_THREADS
+#define FPE_RADAU_THREADS 256
+#endif
 #define FPE_MAX_STRIKES 1024
 #define FPE_MAX_NDOF_V 64      // block size of the block-banded stage LU
 #define FPE_MAX_NDOF_S 160
@@ -35,7 +39,12 @@ enum FpeInfo {
   FPE_INFO_T_FACTOR, FPE_INFO_T_SOLVE, FPE_INFO_T_KRON, FPE_INFO_T_TOTAL,
   FPE_INFO_T_FGJ,    // inside T_FACTOR: pivot-block Gauss-Jordan (kilocycles)
   FPE_INFO_T_FGEMM,  // inside T_FACTOR: L / W products and Schur updates (kilocycles)
-  FPE_INFO_COUNT = 24
+  FPE_INFO_T_SWAIT,  // inside T_SOLVE: waits for the staged sweeps' bulk copies (kilocycles)
+  // inside T_FGJ, each role's own work before the phase's closing barrier
+  // (kilocycles): the real pivot inverse (warp 0), the complex one (warp 1)
+  // and the other Schur updates (warp 2)
+  FPE_INFO_T_GJ_REAL, FPE_INFO_T_GJ_CPLX, FPE_INFO_T_SCHUR,
+  FPE_INFO_COUNT = 32
 };
 
 struct FpeSolveDesc {
@@ -57,6 +66,9 @@ struct FpeSolveDesc {
   int32_t strike_off, n_strikes;
   int32_t save_traj;     // keep every accepted step (stepwise API)
   int32_t traj_cap;      // max saved states
+  int32_t max_steps;     // accepted-step cap (radau.mojo:257-263: 100000)
+  int32_t pad0;
+  int64_t stage_wait;    // SM cycles a staged sweep waits for its copies (<= 0: ~1 s)
   // capacities
   int32_t cap_knot_s, cap_knot_v, cap_grid_s, cap_grid_v, cap_q_s, cap_q_v;
   int32_t cap_dof_s, cap_dof_v;

@@ -67,16 +67,19 @@ struct RadauCtx {
   // work area.
   double* tsm;
   int tsm_cap;  // doubles
+  // Set when a staged sweep's bounded wait gave up: from then on the
+  // intermediate stays out of the stage buffers, where a late copy may land.
+  const int* err;
 };
 
 __device__ __forceinline__ double* vslot(const RadauCtx& C, int k) { return C.work + size_t(k) * C.N; }
 
 // Y_r = sum_t c_t (S_t (x) V_t) X_r, r < nrhs.  Two passes:
 // T_{t,r} = X_r V_t^T, then Y_r = sum_t c_t S_t T_{t,r}.
-__device__ void kron_apply(const RadauCtx& C, const KronTerm* terms, int nt, const double* const* X,
+static __device__ void kron_apply(const RadauCtx& C, const KronTerm* terms, int nt, const double* const* X,
                            double* const* Y, int nrhs) {
   const int nv = C.nv, ns = C.ns, N = C.N;
-  double* T = (C.tsm && nt * nrhs * N <= C.tsm_cap) ? C.tsm : vslot(C, RV_TMP);
+  double* T = (C.tsm && !*C.err && nt * nrhs * N <= C.tsm_cap) ? C.tsm : vslot(C, RV_TMP);
   for (int e = threadIdx.x; e < nt * nrhs * N; e += blockDim.x) {
     const int tr = e / N, idx = e - tr * N;
     const int t = tr / nrhs, r = tr - t * nrhs;
@@ -113,7 +116,7 @@ __device__ void kron_apply(const RadauCtx& C, const KronTerm* terms, int nt, con
 }
 
 struct RadauSmem {
-  unsigned long long pipe_bar[2];  // stage-buffer barriers of the staged block solve
+  unsigned long long pipe_bar[kMaxStageBufs];  // stage-buffer barriers of the staged block solve
   int pipe_err, pipe_pad;
   double red[32 * 8];
   double H[(FPE_GMRES_M + 1) * FPE_GMRES_M];
@@ -125,7 +128,7 @@ struct RadauSmem {
 // scal), or max(1e-6, 1e-3 |t1 - t0|) when that norm is tiny, capped by
 // max_step.  Out of line: it runs once per solve and stays out of the step
 // loop's register allocation.
-__device__ __noinline__ double radau_first_step(const RadauCtx& C, const KronTerm* Kt, const double* y, double* w,
+static __device__ __noinline__ double radau_first_step(const RadauCtx& C, const KronTerm* Kt, const double* y, double* w,
                                                 double sa, double sr, double span, double max_step, double* red) {
   const double* xi[1] = {y};
   double* yo[1] = {w};
@@ -162,6 +165,7 @@ struct RadauKernelArgs {
   double u1, alph, beta, ti13;
   size_t smem_bytes;  // dynamic shared memory of the launch: a solve whose scratch
                       // does not fit in it keeps the scratch in global memory
+  int sweep_bufs;     // most stage buffers a staged sweep may use (2 .. 4)
 };
 
 // The reference's stage constants (radau.mojo:64-75) and the exact ones.
@@ -174,7 +178,7 @@ inline RadauConstants radau_constants(bool exact) {
 }
 
 // Complex operator (ALPH + i BETA) M + h K applied to (xr, xi) (radau.mojo:960-990).
-__device__ void apply_E2(const RadauCtx& C, const KronTerm* Edt, const KronTerm* Mt, double beta,
+static __device__ void apply_E2(const RadauCtx& C, const KronTerm* Edt, const KronTerm* Mt, double beta,
                          const double* xr, const double* xi, double* yr, double* yi, double* t1,
                          double* t2) {
   const double* x2[2] = {xr, xi};
@@ -191,7 +195,7 @@ __device__ void apply_E2(const RadauCtx& C, const KronTerm* Edt, const KronTerm*
 }
 
 template <typename FT>
-__global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
+__global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<FT> A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RadauSmem& S = *reinterpret_cast<RadauSmem*>(smem_raw);
   const FpeSolveDesc d = A.descs[blockIdx.x];
@@ -216,14 +220,13 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
   for (int e = threadIdx.x; e < 4 * ns * 7; e += blockDim.x) fs[e] = D[DL.op_s + e];
   for (int e = threadIdx.x; e < 5 * nv * 7; e += blockDim.x) fv[e] = D[DL.op_v + e];
   if (threadIdx.x == 0) {
-    mbar_init(&S.pipe_bar[0], 1);
-    mbar_init(&S.pipe_bar[1], 1);
+    for (int q = 0; q < kMaxStageBufs; ++q) mbar_init(&S.pipe_bar[q], 1);
     S.pipe_err = 0;
     mbar_init_fence();
   }
   __syncthreads();
   RadauCtx C{ns, nv, N, D + DL.work, fac_shared ? reinterpret_cast<double*>(s_fac) : nullptr,
-             fac_shared ? int(fac_need / sizeof(double)) : 0};
+             fac_shared ? int(fac_need / sizeof(double)) : 0, &S.pipe_err};
   const OpFactors O{ns, nv, fs, fs + ns * 7, fs + 2 * ns * 7, fs + 3 * ns * 7,
                     fv, fv + nv * 7, fv + 2 * nv * 7, fv + 3 * nv * 7, fv + 4 * nv * 7};
   FT* fbase = reinterpret_cast<FT*>(A.farena + d.off_f);
@@ -233,15 +236,22 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
   // Staged sweeps when the stage buffers fit in the (shared) factorization
   // scratch, which is idle while the sweeps run.
   const long long fac_bytes = fac_shared ? (long long)fac_need : 0;
-  const bool staged = fac_bytes >= stage_total_bytes(nv, esz, direct);
+  // As many stage buffers (2 .. A.sweep_bufs) as the scratch holds.
+  const bool staged = fac_bytes >= stage_total_bytes(nv, esz, direct, 2);
   SolveStage SP;
+  SP.nbuf = 2;
+  while (SP.nbuf < min(A.sweep_bufs, kMaxStageBufs) && fac_bytes >= stage_total_bytes(nv, esz, direct, SP.nbuf + 1))
+    ++SP.nbuf;
   SP.slot_r = stage_slot_bytes(nv, esz);
   SP.slot_c = stage_slot_bytes(nv, 2 * esz);
-  SP.buf[0] = reinterpret_cast<unsigned char*>(sbig);
-  SP.buf[1] = SP.buf[0] + 4 * SP.slot_r + (direct ? 4 * SP.slot_c : 0);
-  SP.ring = reinterpret_cast<void*>(SP.buf[1] + 4 * SP.slot_r + (direct ? 4 * SP.slot_c : 0));
+  for (int q = 0; q < kMaxStageBufs; ++q)
+    SP.buf[q] = reinterpret_cast<unsigned char*>(sbig) + size_t(min(q, SP.nbuf)) * stage_bytes(nv, esz, direct);
+  SP.ring = reinterpret_cast<void*>(SP.buf[0] + size_t(SP.nbuf) * stage_bytes(nv, esz, direct));
   SP.bar = S.pipe_bar;
   SP.err = &S.pipe_err;
+  SP.wait_limit = d.stage_wait > 0 ? (long long)d.stage_wait : kBulkWaitLimit;
+  long long t_swait = 0;
+  SP.wait_cycles = &t_swait;
   uint32_t pipe_phase = 0;
   const KronTerm Kt[4] = {{O.Ss, O.B1, 1.0}, {O.Ts, O.B2, 1.0}, {O.As, O.B3, 1.0}, {O.St, O.B4, 1.0}};
   const KronTerm Mt[1] = {{O.As, O.Av, 1.0}};
@@ -267,7 +277,7 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
   // phase timers (SM clock cycles, thread 0 reports)
   const long long t_kernel0 = clock64();
   long long t_factor = 0, t_solve = 0, t_kron = 0;
-  long long t_fsub[2] = {0, 0};  // factorization: Gauss-Jordan, GEMMs
+  long long t_fsub[3] = {0, 0, 0};  // factorization: overlapped phase, products, own role's work
 #define KRON(...)                          \
   do {                                     \
     const long long t_k0 = clock64();      \
@@ -276,6 +286,9 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
   } while (0)
   // block solves ------------------------------------------------------------
   long n_pass_r = 0, n_pass_c = 0;  // sweeps over the real / complex factors
+  // A staged sweep whose bounded wait gave up sets S.pipe_err (uniform after
+  // its closing barrier); the callers leave the Newton iteration and the step
+  // loop ends the solve with FPE_ERR_TIMEOUT.
   auto solve_set = [&](double* xr0, double* xr1, int nr, double* xc_re, double* xc_im, int nc) {
     const long long t_s0 = clock64();
     n_pass_r += nr > 0;
@@ -394,12 +407,15 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
   save_state(t);
 
   long n_loop = 0;
+  // accepted-step cap (radau.mojo:257-263 uses 100000), and a cap on loop
+  // passes that counts rejected steps too
+  const long max_steps = d.max_steps > 0 ? long(d.max_steps) : 100000L;
   while (posneg * (t1 - t) > uround * fmax(fabs(t), fabs(t1))) {
     if (S.pipe_err) {  // a staged sweep's bounded wait gave up: stop this solve
       status = FPE_ERR_TIMEOUT;
       break;
     }
-    if (n_steps > 100000 || ++n_loop > 400000) {
+    if (n_steps > max_steps || ++n_loop > 4 * max_steps + 16) {
       status = FPE_ERR_MAX_STEPS;
       break;
     }
@@ -422,8 +438,12 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
       FT* scr_r = reinterpret_cast<FT*>(sbig);
       Cx<FT>* scr_c = reinterpret_cast<Cx<FT>*>(
           (reinterpret_cast<uintptr_t>(scr_r + fpe_fac_scratch_elems(nv)) + 15) & ~uintptr_t(15));
-      if (!blu_factor_pair<FT>(LR, direct ? &LC : nullptr, scr_r, scr_c, t_fsub)) status = FPE_ERR_SINGULAR;
+      const bool fac_ok = blu_factor_pair<FT>(LR, direct ? &LC : nullptr, scr_r, scr_c, t_fsub);
       t_factor += clock64() - t_f0;
+      if (!fac_ok) {  // a zero or non-finite pivot: no step can use these factors
+        status = FPE_ERR_SINGULAR;
+        break;
+      }
       ++n_lu;
       h_lu = h;
       E1t[0] = {O.As, O.Av, U1};
@@ -550,6 +570,7 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
             const double* Vij = vslot(C, RV_VI + j);
             apply_E2(C, Edt, Mt, BETA, Vrj, Vij, wr, wi, res, res2);
             solve_real2(wr, wi);
+            if (S.pipe_err) break;
             ++n_gmres;
             for (int k = 0; k <= j; ++k) {  // modified Gram-Schmidt, real inner product
               const double* Vrk = vslot(C, RV_VR + k);
@@ -624,6 +645,10 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
           }
           __syncthreads();
         }
+      }
+      if (S.pipe_err) {
+        newt_fail = true;
+        break;
       }
       ++newt;
       ++n_newton;
@@ -701,6 +726,10 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
     for (int e = threadIdx.x; e < N; e += blockDim.x) rerr[e] = MCONT[e] - h * w[e];
     __syncthreads();
     solve_real(err, rerr);
+    if (S.pipe_err) {
+      status = FPE_ERR_TIMEOUT;
+      break;
+    }
     double pe = 0.0;
     for (int e = threadIdx.x; e < N; e += blockDim.x) {
       const double s = sa + sr * fabs(y[e]);
@@ -719,6 +748,10 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
       for (int e = threadIdx.x; e < N; e += blockDim.x) rerr[e] = MCONT[e] - h * w[e];
       __syncthreads();
       solve_real(err, rerr);
+      if (S.pipe_err) {
+        status = FPE_ERR_TIMEOUT;
+        break;
+      }
       pe = 0.0;
       for (int e = threadIdx.x; e < N; e += blockDim.x) {
         const double s = sa + sr * fabs(y[e]);
@@ -727,7 +760,7 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
       en = sqrt(block_sum1(pe, S.red) / double(N));
       if (en < 1e-10) en = 1e-10;
     }
-    if (!(en == en)) {
+    if (!isfinite(en)) {  // NaN or Inf in the error estimate
       status = FPE_ERR_NONFINITE;
       break;
     }
@@ -784,7 +817,11 @@ __global__ void __launch_bounds__(FPE_BLOCK, 1) k_radau(RadauKernelArgs<FT> A) {
     info[FPE_INFO_T_TOTAL] = int((clock64() - t_kernel0) >> 10);
     info[FPE_INFO_T_FGJ] = int(t_fsub[0] >> 10);
     info[FPE_INFO_T_FGEMM] = int(t_fsub[1] >> 10);
+    info[FPE_INFO_T_SWAIT] = int(t_swait >> 10);
+    info[FPE_INFO_T_GJ_REAL] = int(t_fsub[2] >> 10);
   }
+  if (threadIdx.x == 32) info[FPE_INFO_T_GJ_CPLX] = int(t_fsub[2] >> 10);
+  if (threadIdx.x == 64) info[FPE_INFO_T_SCHUR] = int(t_fsub[2] >> 10);
 }
 
 }  // namespace fpe

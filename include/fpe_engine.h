@@ -173,6 +173,17 @@ typedef struct FpeBatchOptions {
                             objective's undiscounted sum over the quadrature points with
                             half-spacing weights, 1 at both ends
                             (src/engines/calibrator/objective.mojo:26-50) */
+    int32_t max_steps;   /* accepted Radau steps before a solve ends with
+                            FPE_STATUS_MAX_STEPS (<= 0 -> 100000, the reference cap,
+                            src/numerics/ode/radau.mojo:257-263) */
+    int32_t fp64_retry;  /* precision 1 only: a solve that ends with a solver failure
+                            (FPE_STATUS_SINGULAR .. FPE_STATUS_TIMEOUT) is solved again
+                            with FP64 factors and that attempt's price and status are
+                            reported; 0 or 1 on (default), < 0 off */
+    int64_t stage_wait_cycles; /* SM clock cycles a staged block solve waits for its
+                            factor copies before the solve ends with FPE_STATUS_TIMEOUT
+                            (<= 0 -> about one second); the FP64 retry always uses the
+                            default.  A short limit exercises the failure path */
 } FpeBatchOptions;
 
 /** Status codes written per strike slot of a batch. */
@@ -217,6 +228,22 @@ extern int32_t fpe_plan_stats(FpePlan* plan, int64_t* out);
 extern int32_t fpe_plan_kernel_times(FpePlan* plan, void* cuda_stream, float* ms);
 /** Number of strike results and of device solves in the plan. */
 extern int32_t fpe_plan_sizes(FpePlan* plan, int32_t* n_results, int32_t* n_solves);
+/** Solves of the last fpe_plan_results call that were solved again with FP64
+ *  factors after a mixed-precision failure (opt->fp64_retry), or < 0. */
+extern int32_t fpe_plan_retried(FpePlan* plan);
+/** Number of words per solve in fpe_plan_solve_info. */
+#define FPE_SOLVE_INFO_WORDS 32
+/** Per-solve counters of the plan's last run, FPE_SOLVE_INFO_WORDS words per
+ *  solve in the plan's solve order (longest estimated solve first): 0 status,
+ *  7-8 dofs (s, v), 9 accepted, 10 rejected, 11 Newton, 12 GMRES, 13 LU
+ *  factorizations, 14 ADMM iterations, 15 / 17 real / complex sweeps,
+ *  18-21 SM kilo-cycles in factorizations, block solves, Kronecker products
+ *  and in total, 22-23 the factorization's pivot inverses and block
+ *  products, 24 the sweeps' waits for their factor copies, 25-27 the
+ *  overlapped factorization phase's own work of the real pivot inverse, the
+ *  complex pivot inverse and the other Schur updates.  out holds
+ *  n_solves * FPE_SOLVE_INFO_WORDS words.  Returns n_solves, < 0 on error. */
+extern int32_t fpe_plan_solve_info(FpePlan* plan, int32_t* out);
 extern void fpe_plan_destroy(FpePlan* plan);
 
 /** One-call batch: plan, run, results, destroy. */
@@ -244,22 +271,29 @@ extern int32_t fpe_device_available(void);
 /** Returned by fpe_price_noalloc when a contract's grids need more scratch than
  *  its static array holds (or n_strikes is outside 1..1024). */
 #define FPE_NOALLOC_ERR_SIZE (-2)
+/** Returned by fpe_price_noalloc when cuda_stream is being captured into a
+ *  CUDA graph; nothing was enqueued and the capture is left intact. */
+#define FPE_NOALLOC_ERR_CAPTURE (-3)
 
 /** Price one contract without allocating any memory.
  *
  *  No counterpart in the reference (which allocates per call).  For callers
- *  that cannot allocate device memory while pricing: code running during CUDA
- *  stream capture, hosts whose GPU memory budget is fixed at start-up, and
- *  plug-ins inside an application that owns the device memory pool.  All
- *  device scratch comes from one static device array of 64 MiB, held by every
- *  GPU that loads the library until exit; a contract whose grids need more
- *  (large n_s x n_v) is rejected with FPE_NOALLOC_ERR_SIZE and its status
- *  slots set to FPE_STATUS_CAPACITY.  The first call on a device resolves the
- *  array's device address (make it before any stream capture).  Calls share
- *  the array: overlapping calls on one device race and must be serialized by
- *  the caller.  prices / status hold n_strikes values (host memory); knock-ins
- *  use in-out parity; opt->greeks must be 0.  Runs on cuda_stream (NULL: the
- *  library's stream) and waits for it.  Returns 0, a status code, or < 0. */
+ *  that cannot allocate device memory while pricing: hosts whose GPU memory
+ *  budget is fixed at start-up, and plug-ins inside an application that owns
+ *  the device memory pool.  All device scratch comes from one static device
+ *  array of 64 MiB, held by every GPU that loads the library until exit; a
+ *  contract whose grids need more (large n_s x n_v) is rejected with
+ *  FPE_NOALLOC_ERR_SIZE and its status slots set to FPE_STATUS_CAPACITY.  The
+ *  first call on each device (the current one) sets that device up: the
+ *  array's device address, a stream of its own, the kernels' shared-memory
+ *  limits.  Calls share the array: overlapping calls on one device race and
+ *  must be serialized by the caller.  The call copies prices / status
+ *  (n_strikes values, host memory) back and waits for its stream, so it cannot
+ *  run on a stream under graph capture: such a stream gives
+ *  FPE_NOALLOC_ERR_CAPTURE before anything is enqueued.  Knock-ins use in-out
+ *  parity; opt->greeks must be 0; opt->fp64_retry is not applied.  Runs on
+ *  cuda_stream (NULL: the device's own stream).  Returns 0, a status code, or
+ *  < 0. */
 extern int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatchOptions* opt,
                                  double* prices, int32_t* status, void* cuda_stream);
 

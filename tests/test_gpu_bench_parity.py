@@ -1,0 +1,90 @@
+"""Parity on the benchmarked workloads: the CUDA path against the CPU FP64
+oracle run now on the same contracts, the same discretization (sinh knots,
+span Gauss-Legendre quadrature), the same Radau tolerance and the same
+algorithm (direct complex stage solve, exact Radau IIA constants).
+
+- The batched European workload: two contracts of each of the nine grid
+  classes (n_s in {32, 48, 64} x n_v in {16, 24, 32}) of the bench's seeded
+  256-contract batch.
+- The knock-in workload: in-out parity (two solves per price, one on the
+  domain truncated at the barrier), eight contracts of the bench's seeded
+  barrier batch, grids up to 96 x 48.
+
+Relative error = |p - p_oracle| / max(|p_oracle|, 1e-6 S0), the metric's
+definition.  Bounds: FP64 factors 1e-7 (the same step sequence as the oracle;
+what is left is the IC projection's ADMM tolerance); FP32 factors 1e-4 (the
+metric's gate: the FP32 preconditioner changes the Newton iterates, so the
+step sequence and with it the time-discretization error of rtol 1e-6 differ
+slightly).
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+RTOL = 1e-6
+FLOOR = 1e-6 * 100.0
+
+
+def _opts(fpe, precision):
+    return fpe.BatchOptions(disc=1, precision=precision, rtol=RTOL, atol=RTOL * 1e-2, complex_solve=2,
+                            radau_constants=2)
+
+
+def _oracle(oracle, P, I):
+    opt = oracle.options(disc=1, rtol=RTOL, atol=RTOL * 1e-2, complex_direct=1, radau_constants=2)
+    return oracle.price_batch(P, I, opt, n_threads=os.cpu_count() or 1)
+
+
+def _rel(p, ref):
+    return np.abs(p - ref) / np.maximum(np.abs(ref), FLOOR)
+
+
+def bench_class_sample(I, per_class=2):
+    """The first `per_class` contracts of each (n_s, n_v) class, in batch order."""
+    idx = []
+    for ns in (32, 48, 64):
+        for nv in (16, 24, 32):
+            idx += list(np.flatnonzero((I[:, 0] == ns) & (I[:, 1] == nv))[:per_class])
+    return np.array(sorted(idx))
+
+
+def test_batched_workload_vs_oracle(engine, oracle):
+    import bench
+
+    fpe = engine
+    P, I = bench.make_batch(bench.N_CONTRACTS, 0)
+    idx = bench_class_sample(I)
+    assert len(idx) == 18
+    Ps, Is = P[idx], I[idx]
+    ref = _oracle(oracle, Ps, Is)
+    p64, s64 = fpe.price_batch(Ps, Is, _opts(fpe, 0))
+    p32, s32 = fpe.price_batch(Ps, Is, _opts(fpe, 1))
+    assert (s64 == 0).all() and (s32 == 0).all()
+    assert _rel(p64, ref).max() < 1e-7, _rel(p64, ref)
+    assert _rel(p32, ref).max() < 1e-4, _rel(p32, ref)
+
+
+def test_knock_in_workload_vs_oracle(engine, oracle):
+    import bench
+
+    fpe = engine
+    P, I = bench.make_barrier_batch(1024, 0)
+    big = np.flatnonzero((I[:, 0] == 96) & (I[:, 1] == 48))[:1]
+    rest = [j for j in range(0, 1024, 37) if I[j, 0] <= 64 and I[j, 1] <= 32][:7]
+    idx = np.concatenate([big, rest]).astype(int)
+    assert len(idx) == 8 and set(I[idx, 2]) == {0, 5}
+    Ps, Is = P[idx], I[idx]
+    ref = _oracle(oracle, Ps, Is)
+    p64, s64 = fpe.price_batch(Ps, Is, _opts(fpe, 0))
+    p32, s32 = fpe.price_batch(Ps, Is, _opts(fpe, 1))
+    assert (s64 == 0).all() and (s32 == 0).all()
+    assert _rel(p64, ref).max() < 1e-7, _rel(p64, ref)
+    assert _rel(p32, ref).max() < 1e-4, _rel(p32, ref)
