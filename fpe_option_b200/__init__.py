@@ -450,6 +450,8 @@ class BatchOptions:
     max_steps: int = 0       # <= 0: 100000 accepted steps (the reference cap)
     fp64_retry: int = 0      # precision 1: re-solve failed solves with FP64 factors (0/1 on, < 0 off)
     stage_wait_cycles: int = 0  # <= 0: ~1 s bounded wait per staged sweep stage
+    block_split: int = 0     # stage-LU blocks: 0 auto, 1 nv x nv, 2 (nv/2) x (nv/2)
+    sweep_buffers: int = 0   # staged-sweep buffers: 0 auto, 2..4
 
     def to_c(self) -> _lib.FpeBatchOptions:
         o = _lib.FpeBatchOptions()
@@ -464,6 +466,7 @@ class BatchOptions:
         o.max_step, o.first_step, o.price_rule = self.max_step, self.first_step, self.price_rule
         o.max_steps, o.fp64_retry = self.max_steps, self.fp64_retry
         o.stage_wait_cycles = self.stage_wait_cycles
+        o.block_split, o.sweep_buffers = self.block_split, self.sweep_buffers
         return o
 
 

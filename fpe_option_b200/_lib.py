@@ -56,7 +56,7 @@ class FpeBatchOptions(C.Structure):
                 ("greeks", i32), ("rel_s", d), ("rel_v", d), ("complex_solve", i32),
                 ("radau_constants", i32), ("max_step", d), ("first_step", d),
                 ("price_rule", i32), ("max_steps", i32), ("fp64_retry", i32),
-                ("stage_wait_cycles", i64)]
+                ("stage_wait_cycles", i64), ("block_split", i32), ("sweep_buffers", i32)]
 
 
 # Every symbol declared in include/*.h.

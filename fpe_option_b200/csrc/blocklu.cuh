@@ -2,15 +2,21 @@
 //
 // E = a M + h K (real a) or (ALPH + i BETA) M + h K (complex shift), with
 // M = As (x) Av and K = Ss (x) B1 + Tss (x) B2 + As (x) B3 + Ss^T (x) B4 in
-// s-major order, is block-banded: nv x nv blocks (i, k), |i - k| <= 3.
+// s-major order (index i nv + j), is banded: entries couple s-dofs |i - k| <= 3
+// and v-dofs |j - l| <= 3.  It is stored block-banded with block size
+// b = nv / m (m = 1 or 2): nb = ns m block rows, bw = 4 m - 1 off-diagonal
+// blocks on each side (m = 1: the nv x nv blocks of one s-coupling, bw = 3;
+// m = 2: half-width blocks, bw = 7).  Both hold the same band (4 nv wide) and
+// cost the same flops; smaller blocks need less scratch and shorten each
+// pivot inverse, larger ones need fewer sequential steps.
 // Block Gaussian elimination without inter-block pivoting (the pivot blocks
 // are D-scaled and diagonally dominated by a M for the step sizes Radau uses;
 // each pivot block is inverted by Gauss-Jordan with partial pivoting):
-//   F[i][kk], kk = k - i + 3:
-//     kk < 3 : L_{i,k} = E_{i,k} P_k^{-1}
-//     kk = 3 : P_i^{-1}
-//     kk > 3 : W_{i,k} = P_i^{-1} U_{i,k}
-// A solve is then 2 ns dense block-GEMV steps (one barrier each):
+//   F[i][kk], kk = k - i + bw:
+//     kk < bw : L_{i,k} = E_{i,k} P_k^{-1}
+//     kk = bw : P_i^{-1}
+//     kk > bw : W_{i,k} = P_i^{-1} U_{i,k}
+// A solve is then 2 nb dense block-GEMV steps (one barrier each):
 //   forward  y_i = b_i - sum_k L_{i,i-k} y_{i-k},   z_i = P_i^{-1} y_i
 //   backward x_i = z_i - sum_k W_{i,i+k} x_{i+k}
 // Storage FT = float (FP32 factors, FP64 accumulation) or double; complex
@@ -102,17 +108,22 @@ struct OpFactors {
   const double *Av, *B1, *B2, *B3, *B4; // v
 };
 
-// Block-banded storage of one stage matrix: block row i holds 7 blocks of
-// nv x nv, kk = 0..6 for block columns i - 3 .. i + 3, each at a stride of
-// fpe_block_stride(nv) elements.  Before and during the factorization a block
-// is row-major; the final factor blocks (L in kk 0-2, P^-1 in kk 3, W = P^-1 U
-// in kk 4-6) are stored transposed (element (j, m) at m nv + j), so that the
-// sweeps read each block column-wise with one output row per thread.
+// Block-banded storage of one stage matrix: block row i holds 2 bw + 1 blocks
+// of b x b, kk = 0 .. 2 bw for block columns i - bw .. i + bw, each at a
+// stride of fpe_block_stride(b) elements.  Before and during the
+// factorization a block is row-major; the final factor blocks (L in kk < bw,
+// P^-1 in kk = bw, W = P^-1 U in kk > bw) are stored transposed (element
+// (j, m) at m b + j), so that the sweeps read each block column-wise with one
+// output row per thread.
 template <typename ET>
 struct BlockLU {
   ET* F;
-  int ns, nv, bs;
-  __device__ __forceinline__ ET* blk(int i, int kk) const { return F + (size_t(i) * 7 + kk) * bs; }
+  int nb;  // block rows (ns m)
+  int b;   // block size (nv / m)
+  int bs;  // element stride between blocks
+  int bw;  // off-diagonal blocks per side (4 m - 1)
+  int nv;  // v-dofs of the grid
+  __device__ __forceinline__ ET* blk(int i, int kk) const { return F + (size_t(i) * (2 * bw + 1) + kk) * bs; }
 };
 
 // E = (a_re + i a_im) M + h K into the block storage (a_im ignored for real ET).
@@ -120,26 +131,30 @@ template <typename ET>
 __device__ void blu_assemble(const OpFactors& O, const BlockLU<ET>& L, double a_re, double a_im,
                              double h) {
   // Block by block: the blocks of a block row whose column lies outside the
-  // matrix (k < 0 or k >= ns) are never read, by the factorization or by the
-  // sweeps, and are not written; the padding after a block's nv^2 entries is
-  // not read either.  Row and column of entry e come from the exact float
-  // reciprocal (e < 2^16), not from integer divisions.
-  const int ns = O.ns, nv = O.nv, bs = L.bs, nn = nv * nv;
-  const float rnv = 1.0f / float(nv);
-  for (int blk = 0; blk < ns * 7; ++blk) {
-    const int i = blk / 7, kk = blk - 7 * i;
-    const int k = i + kk - 3;
-    if (k < 0 || k >= ns) continue;
-    const double as = O.As[blk], ss = O.Ss[blk], ts = O.Ts[blk], st = O.St[blk];
+  // matrix (k < 0 or k >= nb) are never read, by the factorization or by the
+  // sweeps, and are not written; the padding after a block's b^2 entries is
+  // not read either.  Rows and columns come from the exact float reciprocal
+  // (arguments below 2^16), not from integer divisions.
+  const int nb = L.nb, b = L.b, nv = O.nv, bs = L.bs, bw = L.bw, w = 2 * bw + 1, nn = b * b;
+  const float rb = 1.0f / float(b), rnv = 1.0f / float(nv);
+  for (int blk = 0; blk < nb * w; ++blk) {
+    const int i = blk / w, kk = blk - w * i;
+    const int k = i + kk - bw;
+    if (k < 0 || k >= nb) continue;
     ET* B = L.F + size_t(blk) * bs;
     for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-      const int j = int((float(e) + 0.5f) * rnv), l = e - j * nv;
-      const int dl = l - j + 3;
+      const int jj = int((float(e) + 0.5f) * rb), ll = e - jj * b;
+      // global row r = i b + jj = si nv + vj and column c = k b + ll = sk nv + vl
+      const int r = i * b + jj, c = k * b + ll;
+      const int si = int((float(r) + 0.5f) * rnv), vj = r - si * nv;
+      const int sk = int((float(c) + 0.5f) * rnv), vl = c - sk * nv;
+      const int ds = sk - si + 3, dl = vl - vj + 3;
       double m = 0.0, kv = 0.0;
-      if (dl >= 0 && dl < 7) {
-        const int vb = j * 7 + dl;
+      if (ds >= 0 && ds < 7 && dl >= 0 && dl < 7) {
+        const int sb = si * 7 + ds, vb = vj * 7 + dl;
+        const double as = O.As[sb];
         m = as * O.Av[vb];
-        kv = ss * O.B1[vb] + ts * O.B2[vb] + as * O.B3[vb] + st * O.B4[vb];
+        kv = O.Ss[sb] * O.B1[vb] + O.Ts[sb] * O.B2[vb] + as * O.B3[vb] + O.St[sb] * O.B4[vb];
       }
       if constexpr (!IsCx<ET>::v) {
         st_elem(B[e], a_re * m + h * kv);
@@ -206,16 +221,17 @@ __device__ __forceinline__ double fmag(Cx<T> a) {
 // --------------------------------------------------------------------------
 // Stage-matrix factorization scratch (one system, ET elements).
 //
-// Blocks are staged with a padded width nvp = nv rounded up to 4 so that every
-// tile operand is a 16-byte vector load.  GEMM left operands are stored
-// transposed (k-major, row stride ldt = nvp + 4: the transposed staging
-// writes spread over 8 banks), right operands row-major (stride nvp).
-//   aug  nv x (nv + 1)   in-place Gauss-Jordan array of the pivot block
-//   Pi   nvp x nvp       P^-1, row-major        (right operand of L = E P^-1)
-//   PiT  nvp x ldt       P^-1, transposed       (left operand of W = P^-1 U)
-//   EbT  3 x nvp x ldt   E_{i+1+r, i}, transposed
-//   LbT  3 x nvp x ldt   L_{i+1+r, i} = E P^-1, transposed (left operand of the Schur update)
-//   Ub   3 x nvp x nvp   U_{i, i+1+c}, row-major
+// Blocks (b x b; b is called nv inside the scratch) are staged with a padded
+// width nvp = b rounded up to 4 so that every tile operand is a 16-byte vector
+// load.  GEMM left operands are stored transposed (k-major, row stride
+// ldt = nvp + 4: the transposed staging writes spread over 8 banks), right
+// operands row-major (stride nvp).
+//   aug  nv x (nv + 1)    in-place Gauss-Jordan array of the pivot block
+//   Pi   nvp x nvp        P^-1, row-major        (right operand of L = E P^-1)
+//   PiT  nvp x ldt        P^-1, transposed       (left operand of W = P^-1 U)
+//   EbT  bw x nvp x ldt   E_{i+1+r, i}, transposed
+//   LbT  bw x nvp x ldt   L_{i+1+r, i} = E P^-1, transposed (left operand of the Schur update)
+//   Ub   bw x nvp x nvp   U_{i, i+1+c}, row-major
 //   pinv nvp (inverse pivot of each column), then the pivot rows prow_of and
 //   their columns q_of (int)
 // --------------------------------------------------------------------------
@@ -227,8 +243,8 @@ struct FacScratch {
   int* q_of;     // column whose pivot row is r
   int nv, nvp, ldt, w1;
   bool shared;   // scratch in shared memory (async staging possible)
-  __device__ void init(ET* base, int nv_) {
-    nv = nv_;
+  __device__ void init(ET* base, int b, int bw) {
+    nv = b;
     shared = __isShared(base) != 0;
     nvp = fpe_fac_nvp(nv);
     ldt = nvp + 4;
@@ -238,9 +254,9 @@ struct FacScratch {
     Pi = aug + ((nv * (nv + 1) + 3) & ~3);
     PiT = Pi + p * p;
     EbT = PiT + p * t;
-    LbT = EbT + 3 * p * t;
-    Ub = LbT + 3 * p * t;
-    pinv = Ub + 3 * p * p;
+    LbT = EbT + bw * p * t;
+    Ub = LbT + bw * p * t;
+    pinv = Ub + bw * p * p;
     prow_of = reinterpret_cast<int*>(pinv + p);
     q_of = prow_of + p;
   }
@@ -374,7 +390,7 @@ __device__ void fac_stage_impl(const BlockLU<ET>& L, FacScratch<ET>& S, int i, i
   const int nv = S.nv, nn = nv * nv, w1 = S.w1, p = S.nvp, t = S.ldt;
   const float rnv = 1.0f / float(nv);
   if (pivot) {
-    const ET* P = L.blk(i, 3);
+    const ET* P = L.blk(i, L.bw);
     for (int e = threadIdx.x; e < nn; e += blockDim.x) {
       int r, c;
       rc_of(e, nv, rnv, r, c);
@@ -387,8 +403,8 @@ __device__ void fac_stage_impl(const BlockLU<ET>& L, FacScratch<ET>& S, int i, i
   }
   if (rest) {
     for (int cc = 0; cc < nr; ++cc) {
-      const ET* U = L.blk(i, 4 + cc);
-      const ET* E = L.blk(i + 1 + cc, 2 - cc);
+      const ET* U = L.blk(i, L.bw + 1 + cc);
+      const ET* E = L.blk(i + 1 + cc, L.bw - 1 - cc);
       ET* ub = S.Ub + cc * p * p;
       ET* et = S.EbT + cc * p * t;
       for (int e = threadIdx.x; e < nn; e += blockDim.x) {
@@ -496,7 +512,7 @@ template <typename ET>
 __device__ void fac_extract(const BlockLU<ET>& L, FacScratch<ET>& S, int i) {
   const int nv = S.nv, w1 = S.w1, p = S.nvp, t = S.ldt;
   const float rnv = 1.0f / float(nv);
-  ET* g = L.blk(i, 3);
+  ET* g = L.blk(i, L.bw);
   // k varying fastest: the transposed factor store and PiT are contiguous
   for (int e = threadIdx.x; e < nv * nv; e += blockDim.x) {
     int l, k;
@@ -536,7 +552,7 @@ __device__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
     ET* dst;
     if (job < nr) {
       tile_mm<ET, false>(S.EbT + job * p * t, t, S.Pi, p, nv, j0, l0, acc);
-      dst = L.blk(i + 1 + job, 2 - job);
+      dst = L.blk(i + 1 + job, L.bw - 1 - job);
       ET* lt = S.LbT + job * p * t;
 #pragma unroll
       for (int n = 0; n < kTileN; ++n) {
@@ -548,7 +564,7 @@ __device__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
     } else {
       const int cc = job - nr;
       tile_mm<ET, false>(S.PiT, t, S.Ub + cc * p * p, p, nv, j0, l0, acc);
-      dst = L.blk(i, 4 + cc);
+      dst = L.blk(i, L.bw + 1 + cc);
     }
     if (vec && j0 + TM <= nv) {
 #pragma unroll
@@ -586,7 +602,7 @@ __device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int n
     const int jq = q / ntile, tt = q - jq * ntile, job = job_lo + jq;
     const int j0 = (tt / tc) * TM, l0 = (tt - (tt / tc) * tc) * kTileN;
     const int rr = job / nr, cc = job - rr * nr;
-    ET* E = L.blk(i + 1 + rr, cc - rr + 3);
+    ET* E = L.blk(i + 1 + rr, cc - rr + L.bw);
     ET acc[TM][kTileN];
 #pragma unroll
     for (int m = 0; m < TM; ++m)
@@ -612,15 +628,15 @@ __device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int n
 
 // Factor the real stage matrix (and, when LC is given, the complex one in
 // lockstep so both share every barrier).  scr_r / scr_c: scratch of
-// fpe_fac_scratch_elems(nv) elements each.
+// fpe_fac_scratch_elems(b, bw) elements each.
 template <typename FT>
 __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC, FT* scr_r,
                                 Cx<FT>* scr_c, long long (&tcyc)[3]) {
-  const int ns = LR.ns;
+  const int ns = LR.nb, bw = LR.bw;  // block rows, off-diagonal blocks
   FacScratch<FT> SR;
-  SR.init(scr_r, LR.nv);
+  SR.init(scr_r, LR.b, bw);
   FacScratch<Cx<FT>> SC;
-  if (LC) SC.init(scr_c, LR.nv);
+  if (LC) SC.init(scr_c, LR.b, bw);
   bool ok = true;
   const int warp = threadIdx.x >> 5;
   // Lookahead: block row i computes the next pivot block first (Schur job 0,
@@ -632,8 +648,8 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
   if (ns <= 0) return true;
   {
     const long long t0 = clock64();
-    fac_stage<FT>(LR, SR, 0, min(3, ns - 1));
-    if (LC) fac_stage<Cx<FT>>(*LC, SC, 0, min(3, ns - 1));
+    fac_stage<FT>(LR, SR, 0, min(bw, ns - 1));
+    if (LC) fac_stage<Cx<FT>>(*LC, SC, 0, min(bw, ns - 1));
     __syncthreads();
     if (warp == 0) ok &= fac_gj_warp<FT>(SR);
     else if (warp == 1 && LC) ok &= fac_gj_warp<Cx<FT>>(SC);
@@ -641,7 +657,7 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
     tcyc[0] += clock64() - t0;
   }
   for (int i = 0; i < ns; ++i) {
-    const int nr = min(i + 3, ns - 1) - i;
+    const int nr = min(i + bw, ns - 1) - i;
     if (i > 0) {  // U and E blocks of row i (its pivot block is already inverted)
       fac_stage<FT>(LR, SR, i, nr, false, true);
       if (LC) fac_stage<Cx<FT>>(*LC, SC, i, nr, false, true);
@@ -750,8 +766,9 @@ __device__ __forceinline__ Cx<double> grp_dot<Cx<double>, Cx<double>>(const Cx<d
 // shuffle reductions (real systems carry a zero imaginary part).
 template <typename FT>
 __device__ void blu_solve(const SolveSet<FT>& S) {
-  const int ns = S.R ? S.R->ns : S.Cf->ns;
-  const int nv = S.R ? S.R->nv : S.Cf->nv;
+  const int ns = S.R ? S.R->nb : S.Cf->nb;  // block rows
+  const int nv = S.R ? S.R->b : S.Cf->b;    // block size
+  const int bw = S.R ? S.R->bw : S.Cf->bw;
   const int rows = (S.nr + S.nc) * nv;
   int G = 32;
   while (G > 1 && rows * G > int(blockDim.x)) G >>= 1;
@@ -776,20 +793,20 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
       const BlockLU<FT>& L = *S.R;
       const double* x = S.xr[sys];
       if (i < ns)
-        for (int k = 1; k <= 3 && i - k >= 0; ++k)
-          ar += grp_dot<FT, double>(L.blk(i, 3 - k) + j, x + (i - k) * nv, nullptr, nv, gl, G);
-      if (i > 0) zr = grp_dot<FT, double>(L.blk(i - 1, 3) + j, x + (i - 1) * nv, nullptr, nv, gl, G);
+        for (int k = 1; k <= bw && i - k >= 0; ++k)
+          ar += grp_dot<FT, double>(L.blk(i, bw - k) + j, x + (i - k) * nv, nullptr, nv, gl, G);
+      if (i > 0) zr = grp_dot<FT, double>(L.blk(i - 1, bw) + j, x + (i - 1) * nv, nullptr, nv, gl, G);
     } else if (is_c) {
       const BlockLU<Cx<FT>>& L = *S.Cf;
       if (i < ns)
-        for (int k = 1; k <= 3 && i - k >= 0; ++k) {
-          const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i, 3 - k) + j, S.xc_re + (i - k) * nv,
+        for (int k = 1; k <= bw && i - k >= 0; ++k) {
+          const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i, bw - k) + j, S.xc_re + (i - k) * nv,
                                                            S.xc_im + (i - k) * nv, nv, gl, G);
           ar += d.re;
           ai += d.im;
         }
       if (i > 0) {
-        const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i - 1, 3) + j, S.xc_re + (i - 1) * nv,
+        const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i - 1, bw) + j, S.xc_re + (i - 1) * nv,
                                                          S.xc_im + (i - 1) * nv, nv, gl, G);
         zr = d.re;
         zi = d.im;
@@ -819,12 +836,12 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
     if (is_r) {
       const BlockLU<FT>& L = *S.R;
       const double* x = S.xr[sys];
-      for (int k = 1; k <= 3 && i + k < ns; ++k)
-        ar += grp_dot<FT, double>(L.blk(i, 3 + k) + j, x + (i + k) * nv, nullptr, nv, gl, G);
+      for (int k = 1; k <= bw && i + k < ns; ++k)
+        ar += grp_dot<FT, double>(L.blk(i, bw + k) + j, x + (i + k) * nv, nullptr, nv, gl, G);
     } else if (is_c) {
       const BlockLU<Cx<FT>>& L = *S.Cf;
-      for (int k = 1; k <= 3 && i + k < ns; ++k) {
-        const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i, 3 + k) + j, S.xc_re + (i + k) * nv,
+      for (int k = 1; k <= bw && i + k < ns; ++k) {
+        const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i, bw + k) + j, S.xc_re + (i + k) * nv,
                                                          S.xc_im + (i + k) * nv, nv, gl, G);
         ar += d.re;
         ai += d.im;
@@ -847,16 +864,17 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
 // --------------------------------------------------------------------------
 // Staged fused block solve.
 //
-// The 2 ns + 1 block rows of a solve (forward rows 0..ns, backward rows
-// ns-1..0) stream through nbuf (2 to 4) shared-memory stage buffers by bulk
+// The 2 nb + 1 block rows of a solve (forward rows 0..nb, backward rows
+// nb-1..0) stream through nbuf (2 to 4) shared-memory stage buffers by bulk
 // copies: while the CTA multiplies stage s, stages s + 1 .. s + nbuf - 1 are
 // in flight, and one thread issues stage s + nbuf into the freed buffer after
 // the row's barrier, so each copy has nbuf - 1 stage times to land.  A stage
-// holds the blocks the row needs from each factor (forward row i: L_{i,i-3+g},
-// g < 3, and P^-1_{i-1}; backward row i: W_{i,i+1+g}), one slot per block with
-// a 64-byte gap so that the slots of a complex row group start in alternate
-// bank halves.  The last four solved block segments of every right-hand side
-// stay in a shared ring, so each row reads its x operands from shared memory.
+// holds the blocks the row needs from each factor (forward row i:
+// L_{i,i-bw+g}, g < bw, and P^-1_{i-1}; backward row i: W_{i,i+1+g}), one slot
+// per block with a 64-byte gap so that the slots of a complex row group start
+// in alternate bank halves.  The last bw + 1 solved block segments of every
+// right-hand side stay in a shared ring (a power of two of segments), so each
+// row reads its x operands from shared memory.
 // One thread owns one row of a real system; Gc lanes own one row of the
 // complex system and split its blocks.
 // --------------------------------------------------------------------------
@@ -865,8 +883,9 @@ constexpr int kMaxStageBufs = 4;
 struct SolveStage {
   unsigned char* buf[kMaxStageBufs];  // stage buffers (shared, 16-byte aligned)
   int nbuf;                  // buffers in use (2 .. kMaxStageBufs)
-  void* ring;                // 4 segments x nv per right-hand-side array (nr real, re, im), of the
-                             // sweep's accumulation type (float with FP32 factors, else double)
+  void* ring;                // ring_segments(bw) segments x b per right-hand-side array (nr real,
+                             // re, im), of the sweep's accumulation type (float with FP32
+                             // factors, else double)
   unsigned long long* bar;   // nbuf mbarriers (shared)
   int* err;                  // shared flag: a bounded wait gave up
   int slot_r, slot_c;        // bytes per staged real / complex block slot
@@ -874,30 +893,32 @@ struct SolveStage {
   long long* wait_cycles;    // accumulates this thread's cycles spent in those waits
 };
 
-__host__ __device__ __forceinline__ int stage_slot_bytes(int nv, int esz) {
-  return fpe_block_stride(nv) * esz + 64;
+__host__ __device__ __forceinline__ int stage_slot_bytes(int b, int esz) {
+  return fpe_block_stride(b) * esz + 64;
 }
-// Bytes of one stage buffer for block size nv, element size esz of the real
-// factor, with or without the complex factor.
-__host__ __device__ __forceinline__ int stage_bytes(int nv, int esz, bool cplx) {
-  return 4 * stage_slot_bytes(nv, esz) + (cplx ? 4 * stage_slot_bytes(nv, 2 * esz) : 0);
+// Segments of the sweep's ring: bw + 1 rounded up to a power of two.
+__host__ __device__ __forceinline__ int ring_segments(int bw) { return bw < 4 ? 4 : 8; }
+// Bytes of one stage buffer (bw + 1 slots) for block size b, element size esz
+// of the real factor, with or without the complex factor.
+__host__ __device__ __forceinline__ int stage_bytes(int b, int esz, bool cplx, int bw) {
+  return (bw + 1) * (stage_slot_bytes(b, esz) + (cplx ? stage_slot_bytes(b, 2 * esz) : 0));
 }
-// Bytes of nbuf stage buffers plus the ring.
-__host__ __device__ __forceinline__ int stage_total_bytes(int nv, int esz, bool cplx, int nbuf = 2) {
-  return nbuf * stage_bytes(nv, esz, cplx) + 4 * nv * 4 * 8;
+// Bytes of nbuf stage buffers plus the ring (up to 4 arrays of 8-byte entries).
+__host__ __device__ __forceinline__ int stage_total_bytes(int b, int esz, bool cplx, int bw, int nbuf) {
+  return nbuf * stage_bytes(b, esz, cplx, bw) + ring_segments(bw) * b * 4 * 8;
 }
 
 // Block (row, kk) of stage s and slot g; nullptr when the row has no such block.
 template <typename ET>
 __device__ __forceinline__ const ET* stage_block(const BlockLU<ET>& L, int s, int g) {
-  const int ns = L.ns;
-  if (s <= ns) {
+  const int nb = L.nb, bw = L.bw;
+  if (s <= nb) {
     const int i = s;
-    if (g < 3) return (i < ns && i - 3 + g >= 0) ? L.blk(i, g) : nullptr;
-    return i >= 1 ? L.blk(i - 1, 3) : nullptr;
+    if (g < bw) return (i < nb && i - bw + g >= 0) ? L.blk(i, g) : nullptr;
+    return i >= 1 ? L.blk(i - 1, bw) : nullptr;
   }
-  const int i = 2 * ns - s;
-  return (g < 3 && i + 1 + g < ns) ? L.blk(i, 4 + g) : nullptr;
+  const int i = 2 * nb - s;
+  return (g < bw && i + 1 + g < nb) ? L.blk(i, bw + 1 + g) : nullptr;
 }
 
 // Issues the bulk copies of stage s.  gfence orders the factor's earlier
@@ -907,11 +928,12 @@ template <typename FT>
 __device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s, int b, bool gfence) {
   unsigned long long* bar = P.bar + b;
   unsigned char* dst = P.buf[b];
-  const int nv = S.R ? S.R->nv : S.Cf->nv;
+  const int nv = S.R ? S.R->b : S.Cf->b;  // block size
+  const int ng = (S.R ? S.R->bw : S.Cf->bw) + 1;
   const uint32_t br = uint32_t(fpe_block_stride(nv)) * sizeof(FT);
   const uint32_t bc = 2 * br;
   uint32_t bytes = 0;
-  for (int g = 0; g < 4; ++g) {
+  for (int g = 0; g < ng; ++g) {
     if (S.nr > 0 && stage_block(*S.R, s, g)) bytes += br;
     if (S.nc > 0 && stage_block(*S.Cf, s, g)) bytes += bc;
   }
@@ -922,14 +944,14 @@ __device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s, i
     return;
   }
   mbar_arrive_expect_tx(bar, bytes);
-  for (int g = 0; g < 4; ++g) {
+  for (int g = 0; g < ng; ++g) {
     if (S.nr > 0) {
       const FT* src = stage_block(*S.R, s, g);
       if (src) bulk_g2s(dst + g * P.slot_r, src, br, bar);
     }
     if (S.nc > 0) {
       const Cx<FT>* src = stage_block(*S.Cf, s, g);
-      if (src) bulk_g2s(dst + 4 * P.slot_r + g * P.slot_c, src, bc, bar);
+      if (src) bulk_g2s(dst + ng * P.slot_r + g * P.slot_c, src, bc, bar);
     }
   }
 }
@@ -1019,8 +1041,11 @@ __device__ __forceinline__ void col_dot_c(const Cx<T>* col, const double* xr, co
 template <typename FT>
 __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uint32_t& phase) {
   if (*P.err) return false;
-  const int ns = S.R ? S.R->ns : S.Cf->ns;
-  const int nv = S.R ? S.R->nv : S.Cf->nv;
+  const int ns = S.R ? S.R->nb : S.Cf->nb;  // block rows
+  const int nv = S.R ? S.R->b : S.Cf->b;    // block size
+  const int bw = S.R ? S.R->bw : S.Cf->bw;
+  const int ng = bw + 1;                    // slots per stage
+  const int rmask = ring_segments(bw) - 1;
   const int nstage = 2 * ns + 1;
   const int tid = threadIdx.x;
   // roles
@@ -1035,24 +1060,24 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
   const int cu = is_c ? tid - cbase : 0;
   const int cj = cu / Gc, cg = cu - cj * Gc;
   using RT = FT;  // accumulation / ring type: float with FP32 factors, double with FP64
-  const int nv4 = 4 * nv;
+  const int rlen = (rmask + 1) * nv;  // ring length per right-hand-side array
   RT* ringb = static_cast<RT*>(P.ring);
-  RT* ring_c_re = ringb + S.nr * nv4;
-  RT* ring_c_im = ring_c_re + nv4;
+  RT* ring_c_re = ringb + S.nr * rlen;
+  RT* ring_c_im = ring_c_re + rlen;
 
   // the thread that issues the copies: an idle one when the roles leave one
   const int issuer = (int(blockDim.x) - 1 >= max(nreal, cbase + (S.nc > 0 ? Gc * nv : 0))) ? int(blockDim.x) - 1 : 0;
-  const int nb = P.nbuf;
+  const int nbuf = P.nbuf;
   uint32_t pend = 0;  // buffers with a stage in flight (the issuer's view)
   if (tid == issuer) {
-    for (int q = 0; q < nb && q < nstage; ++q) {
+    for (int q = 0; q < nbuf && q < nstage; ++q) {
       stage_issue<FT>(S, P, q, q, q == 0);
       pend |= 1u << q;
     }
   }
   bool ok = true;
-  int b = 0;  // buffer of stage s: s mod nb
-  for (int s = 0; s < nstage; ++s, b = (b + 1 == nb) ? 0 : b + 1) {
+  int b = 0;  // buffer of stage s: s mod nbuf
+  for (int s = 0; s < nstage; ++s, b = (b + 1 == nbuf) ? 0 : b + 1) {
     const long long tw0 = clock64();
     const bool landed = mbar_wait_bounded(P.bar + b, (phase >> b) & 1u, P.wait_limit);
     *P.wait_cycles += clock64() - tw0;
@@ -1069,41 +1094,47 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
     const int i = fwd ? s : 2 * ns - s;
     if (ok) {
       if (is_r) {
-        const RT* ring = ringb + rsys * nv4;
+        const RT* ring = ringb + rsys * rlen;
         RT a = RT(0), z = RT(0);
         if (fwd) {
-          for (int g = 0; g < 3; ++g)
-            if (i < ns && i - 3 + g >= 0)
-              col_dot(reinterpret_cast<const FT*>(buf + g * P.slot_r) + rj, ring + ((i - 3 + g) & 3) * nv, nv, a);
-          if (i >= 1) col_dot(reinterpret_cast<const FT*>(buf + 3 * P.slot_r) + rj, ring + ((i - 1) & 3) * nv, nv, z);
-          if (i < ns) ringb[rsys * nv4 + (i & 3) * nv + rj] = RT(S.xr[rsys][i * nv + rj] - double(a));
+          // the right-hand side's row is loaded before the products
+          const double xb = i < ns ? S.xr[rsys][i * nv + rj] : 0.0;
+          for (int g = 0; g < bw; ++g)
+            if (i < ns && i - bw + g >= 0)
+              col_dot(reinterpret_cast<const FT*>(buf + g * P.slot_r) + rj, ring + ((i - bw + g) & rmask) * nv, nv,
+                      a);
+          if (i >= 1)
+            col_dot(reinterpret_cast<const FT*>(buf + bw * P.slot_r) + rj, ring + ((i - 1) & rmask) * nv, nv, z);
+          if (i < ns) ringb[rsys * rlen + (i & rmask) * nv + rj] = RT(xb - double(a));
           if (i >= 1) S.zr[rsys][(i - 1) * nv + rj] = double(z);
         } else {
-          for (int g = 0; g < 3; ++g)
+          const double zb = S.zr[rsys][i * nv + rj];
+          for (int g = 0; g < bw; ++g)
             if (i + 1 + g < ns)
-              col_dot(reinterpret_cast<const FT*>(buf + g * P.slot_r) + rj, ring + ((i + 1 + g) & 3) * nv, nv, a);
-          const double x = S.zr[rsys][i * nv + rj] - double(a);
-          ringb[rsys * nv4 + (i & 3) * nv + rj] = RT(x);
+              col_dot(reinterpret_cast<const FT*>(buf + g * P.slot_r) + rj, ring + ((i + 1 + g) & rmask) * nv, nv,
+                      a);
+          const double x = zb - double(a);
+          ringb[rsys * rlen + (i & rmask) * nv + rj] = RT(x);
           S.xr[rsys][i * nv + rj] = x;
         }
       }
       RT ar = RT(0), ai = RT(0), zr = RT(0), zi = RT(0);
       if (is_c) {
-        const unsigned char* cb = buf + 4 * P.slot_r;
-        for (int g = cg; g < 4; g += Gc) {
+        const unsigned char* cb = buf + ng * P.slot_r;
+        for (int g = cg; g < ng; g += Gc) {
           const Cx<FT>* col = reinterpret_cast<const Cx<FT>*>(cb + g * P.slot_c) + cj;
           if (fwd) {
-            if (g < 3) {
-              if (i < ns && i - 3 + g >= 0) {
-                const int seg = ((i - 3 + g) & 3) * nv;
+            if (g < bw) {
+              if (i < ns && i - bw + g >= 0) {
+                const int seg = ((i - bw + g) & rmask) * nv;
                 col_dot_c(col, ring_c_re + seg, ring_c_im + seg, nv, ar, ai);
               }
             } else if (i >= 1) {
-              const int seg = ((i - 1) & 3) * nv;
+              const int seg = ((i - 1) & rmask) * nv;
               col_dot_c(col, ring_c_re + seg, ring_c_im + seg, nv, zr, zi);
             }
-          } else if (g < 3 && i + 1 + g < ns) {
-            const int seg = ((i + 1 + g) & 3) * nv;
+          } else if (g < bw && i + 1 + g < ns) {
+            const int seg = ((i + 1 + g) & rmask) * nv;
             col_dot_c(col, ring_c_re + seg, ring_c_im + seg, nv, ar, ai);
           }
         }
@@ -1118,8 +1149,8 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
       if (is_c && cg == 0) {
         if (fwd) {
           if (i < ns) {
-            ring_c_re[(i & 3) * nv + cj] = RT(S.xc_re[i * nv + cj] - double(ar));
-            ring_c_im[(i & 3) * nv + cj] = RT(S.xc_im[i * nv + cj] - double(ai));
+            ring_c_re[(i & rmask) * nv + cj] = RT(S.xc_re[i * nv + cj] - double(ar));
+            ring_c_im[(i & rmask) * nv + cj] = RT(S.xc_im[i * nv + cj] - double(ai));
           }
           if (i >= 1) {
             S.zc_re[(i - 1) * nv + cj] = double(zr);
@@ -1127,8 +1158,8 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
           }
         } else {
           const double xr = S.zc_re[i * nv + cj] - double(ar), xi = S.zc_im[i * nv + cj] - double(ai);
-          ring_c_re[(i & 3) * nv + cj] = RT(xr);
-          ring_c_im[(i & 3) * nv + cj] = RT(xi);
+          ring_c_re[(i & rmask) * nv + cj] = RT(xr);
+          ring_c_im[(i & rmask) * nv + cj] = RT(xi);
           S.xc_re[i * nv + cj] = xr;
           S.xc_im[i * nv + cj] = xi;
         }
@@ -1139,15 +1170,15 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
       ok = false;
       break;
     }
-    if (tid == issuer && s + nb < nstage) {
-      stage_issue<FT>(S, P, s + nb, b, false);
+    if (tid == issuer && s + nbuf < nstage) {
+      stage_issue<FT>(S, P, s + nbuf, b, false);
       pend |= 1u << b;
     }
   }
   if (!ok && tid == issuer) {
     // let copies still in flight land before the buffers are reused: the full
     // (about one second) limit, whatever the stage waits were given
-    for (int q = 0; q < nb; ++q)
+    for (int q = 0; q < nbuf; ++q)
       if ((pend >> q) & 1u) mbar_wait_bounded(P.bar + q, (phase >> q) & 1u, kBulkWaitLimit);
   }
   __syncthreads();

@@ -124,6 +124,8 @@ struct Opts {
   int max_steps = 0;                        // <= 0: 100000 (radau.mojo:257-263)
   int fp64_retry = 1;                       // re-solve failed mixed solves with FP64 factors
   long long stage_wait = 0;                 // <= 0: about one second
+  int block_split = 0;                      // 0 auto, 1 nv x nv blocks, 2 half-width blocks
+  int sweep_buffers = 0;                    // 0 auto, 2 .. 4
 };
 
 Opts opts_from(const FpeBatchOptions* o, int default_num_insert) {
@@ -154,6 +156,8 @@ Opts opts_from(const FpeBatchOptions* o, int default_num_insert) {
   r.max_steps = o->max_steps > 0 ? o->max_steps : 0;
   r.fp64_retry = o->fp64_retry < 0 ? 0 : 1;
   r.stage_wait = o->stage_wait_cycles > 0 ? (long long)o->stage_wait_cycles : 0;
+  r.block_split = (o->block_split == 1 || o->block_split == 2) ? o->block_split : 0;
+  r.sweep_buffers = (o->sweep_buffers >= 2 && o->sweep_buffers <= 4) ? o->sweep_buffers : 0;
   return r;
 }
 
@@ -259,12 +263,40 @@ struct FpePlan {
   cudaStream_t stream = nullptr;
 };
 
+// Dynamic shared memory of one solve in the Radau kernel: the fixed part
+// (control block and the 1-D operator factors; *base) plus the real and, for
+// the direct complex stage solve, complex factorization scratch of its block
+// split (capacities, so the kernel's own decision from the actual sizes never
+// asks for more).
+static size_t radau_smem_need(const FpeSolveDesc& d, int esz, int cplx, size_t* base) {
+  const int nv = std::min(d.cap_dof_v, FPE_MAX_NDOF_V);
+  const int ns_cap = std::min(d.cap_dof_s, FPE_MAX_NDOF_S);
+  const int m = fpe_blk_split(d.blk_split, nv);
+  const size_t el = size_t(fpe_fac_scratch_elems(nv / m, fpe_blk_bw(m)));
+  *base = sizeof(fpe::RadauSmem) + size_t(4 * ns_cap * 7 + 5 * nv * 7) * 8 + 64;
+  return *base + el * esz + (cplx ? el * 2 * esz + 16 : 0);
+}
+
+// The stage-LU block split of a solve: the caller's choice, else full nv x nv
+// blocks when their factorization scratch fits in shared memory and
+// half-width blocks when it does not (nv = 48 in mixed precision, for one).
+static void resolve_block_split(FpeSolveDesc& d, const Opts& o, int esz, size_t optin) {
+  if (o.block_split) {
+    d.blk_split = o.block_split;
+    return;
+  }
+  d.blk_split = 1;
+  size_t base = 0;
+  if (radau_smem_need(d, esz, o.complex_mode, &base) > optin) d.blk_split = 2;
+}
+
 static int plan_layout(FpePlan* P, int esz) {
   int64_t od = 0, oi = 0, of = 0, ot = 0;
   size_t smem_fit_max = 0, smem_base_max = 0;
   const size_t optin = size_t(ctx().smem_optin > 0 ? ctx().smem_optin : 232448);
   const int cplx = P->o.complex_mode;
   for (auto& d : P->descs) {
+    resolve_block_split(d, P->o, esz, optin);
     d.off_d = od;
     d.off_i = oi;
     d.off_f = of;
@@ -275,13 +307,8 @@ static int plan_layout(FpePlan* P, int esz) {
       d.off_traj = ot;
       ot += d.traj_cap + int64_t(d.traj_cap) * d.cap_dof_s * d.cap_dof_v;
     }
-    const int nv = std::min(d.cap_dof_v, FPE_MAX_NDOF_V);
-    const int ns_cap = std::min(d.cap_dof_s, FPE_MAX_NDOF_S);
-    const int ebytes = cplx ? 2 * esz : esz;  // the complex factor needs the larger scratch
-    size_t base = sizeof(fpe::RadauSmem) + size_t(4 * ns_cap * 7 + 5 * nv * 7) * 8 + 64;
-    size_t sm = base + size_t(fpe_fac_scratch_elems(nv)) * esz +
-                (cplx ? size_t(fpe_fac_scratch_elems(nv)) * 2 * esz + 16 : 0);
-    (void)ebytes;
+    size_t base = 0;
+    const size_t sm = radau_smem_need(d, esz, cplx, &base);
     smem_base_max = std::max(smem_base_max, base);
     if (sm <= optin) smem_fit_max = std::max(smem_fit_max, sm);
   }
@@ -351,12 +378,14 @@ static int plan_launch(FpePlan* P, cudaStream_t s, int from, int to) {
     if (P->o.precision == 0) {
       fpe::RadauKernelArgs<double> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena,
                                      P->d_traj, 0, P->o.complex_mode, P->fac_global,
-                                     rk.u1, rk.alph, rk.beta, rk.ti13, P->radau_smem, FPE_SWEEP_BUFS};
+                                     rk.u1, rk.alph, rk.beta, rk.ti13, P->radau_smem,
+                                     P->o.sweep_buffers ? P->o.sweep_buffers : FPE_SWEEP_BUFS};
       CK(fpe::launch_radau<double>(a, grid, dim3(FPE_RADAU_THREADS), P->radau_smem, s));
     } else {
       fpe::RadauKernelArgs<float> a{P->d_descs, P->d_arena, P->d_iarena, P->d_infos, P->d_farena,
                                     P->d_traj, P->o.refine, P->o.complex_mode, P->fac_global,
-                                    rk.u1, rk.alph, rk.beta, rk.ti13, P->radau_smem, FPE_SWEEP_BUFS};
+                                    rk.u1, rk.alph, rk.beta, rk.ti13, P->radau_smem,
+                                     P->o.sweep_buffers ? P->o.sweep_buffers : FPE_SWEEP_BUFS};
       CK(fpe::launch_radau<float>(a, grid, dim3(FPE_RADAU_THREADS), P->radau_smem, s));
     }
     ++launches;
@@ -1255,6 +1284,7 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
   int64_t od = 0, oi = 0, of = 0;
   size_t smem_max = 0, smem_base = 0, ic = 0;
   for (int k = 0; k < nsolve; ++k) {
+    resolve_block_split(d[k], o, esz, size_t(ND->smem_optin));
     d[k].strike_off = k * nk;
     d[k].off_d = od;
     d[k].off_i = oi;
@@ -1265,12 +1295,9 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
     od += fpe_dlayout(d[k]).total;
     oi += fpe_ilayout(d[k]).total;
     of += fpe_factor_bytes(d[k], esz, o.complex_mode);
-    const int nv = std::min(d[k].cap_dof_v, FPE_MAX_NDOF_V);
-    const int ns_cap = std::min(d[k].cap_dof_s, FPE_MAX_NDOF_S);
-    const size_t b = sizeof(fpe::RadauSmem) + size_t(4 * ns_cap * 7 + 5 * nv * 7) * 8 + 64;
+    size_t b = 0;
+    smem_max = std::max(smem_max, radau_smem_need(d[k], esz, o.complex_mode, &b));
     smem_base = std::max(smem_base, b);
-    smem_max = std::max(smem_max, b + size_t(fpe_fac_scratch_elems(nv)) * esz +
-                                      (o.complex_mode ? size_t(fpe_fac_scratch_elems(nv)) * 2 * esz + 16 : 0));
     ic = std::max(ic, fpe_ic_admm_bytes(d[k].cap_dof_s, d[k].cap_dof_v));
   }
   const size_t off_d = off;
@@ -1310,11 +1337,13 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
   const fpe::RadauConstants rk = fpe::radau_constants(o.radau_exact != 0);
   if (o.precision == 0) {
     fpe::RadauKernelArgs<double> a{g_desc, g_d, g_i, g_info, g_f, nullptr, 0, o.complex_mode,
-                                   fac_global, rk.u1, rk.alph, rk.beta, rk.ti13, radau_smem, FPE_SWEEP_BUFS};
+                                   fac_global, rk.u1, rk.alph, rk.beta, rk.ti13, radau_smem,
+                                   o.sweep_buffers ? o.sweep_buffers : FPE_SWEEP_BUFS};
     CK(fpe::launch_radau<double>(a, grid, dim3(FPE_RADAU_THREADS), radau_smem, s));
   } else {
     fpe::RadauKernelArgs<float> a{g_desc, g_d, g_i, g_info, g_f, nullptr, o.refine, o.complex_mode,
-                                  fac_global, rk.u1, rk.alph, rk.beta, rk.ti13, radau_smem, FPE_SWEEP_BUFS};
+                                  fac_global, rk.u1, rk.alph, rk.beta, rk.ti13, radau_smem,
+                                   o.sweep_buffers ? o.sweep_buffers : FPE_SWEEP_BUFS};
     CK(fpe::launch_radau<float>(a, grid, dim3(FPE_RADAU_THREADS), radau_smem, s));
   }
   fpe::k_payoff<<<grid, block, 0, s>>>(g_desc, g_d, g_i, g_info, g_k, g_p);

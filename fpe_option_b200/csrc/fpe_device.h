@@ -67,7 +67,7 @@ struct FpeSolveDesc {
   int32_t save_traj;     // keep every accepted step (stepwise API)
   int32_t traj_cap;      // max saved states
   int32_t max_steps;     // accepted-step cap (radau.mojo:257-263: 100000)
-  int32_t pad0;
+  int32_t blk_split;     // stage-LU block size nv / blk_split (1 or 2; see fpe_blk_split)
   int64_t stage_wait;    // SM cycles a staged sweep waits for its copies (<= 0: ~1 s)
   // capacities
   int32_t cap_knot_s, cap_knot_v, cap_grid_s, cap_grid_v, cap_q_s, cap_q_v;
@@ -115,20 +115,26 @@ struct FpeILayout {
 #define FPE_HD inline
 #endif
 
-// Stage-factorization scratch of one system, in elements: the pivot block's
-// Gauss-Jordan array nv x (nv + 1), then blocks padded to nvp = nv rounded up
-// to 4 (row-major nvp x nvp, transposed nvp x (nvp + 4)): P^-1 both ways, three
-// transposed E and L blocks, three U blocks, and the pivot bookkeeping (with
-// room to spare).
+// Block structure of the stage LU for nv v-dofs: blocks of b = nv / m with
+// bw = 4 m - 1 off-diagonal blocks per side (m = 1: one s-coupling per block,
+// bw = 3; m = 2: half-width blocks, bw = 7).  m = 2 needs an even nv.
+FPE_HD int fpe_blk_split(int requested, int nv) { return (requested == 2 && nv % 2 == 0 && nv >= 8) ? 2 : 1; }
+FPE_HD int fpe_blk_bw(int m) { return 4 * m - 1; }
+
+// Stage-factorization scratch of one system, in elements, for block size b
+// and bw off-diagonal blocks: the pivot block's Gauss-Jordan array
+// b x (b + 1), then blocks padded to p = b rounded up to 4 (row-major p x p,
+// transposed p x (p + 4)): P^-1 both ways, bw transposed E and L blocks, bw U
+// blocks, and the pivot bookkeeping (with room to spare).
 FPE_HD int fpe_fac_nvp(int nv) { return (nv + 3) & ~3; }
-// Element stride between the nv x nv blocks of a stored stage factor: nv^2
+// Element stride between the b x b blocks of a stored stage factor: b^2
 // rounded up to 4, so every block starts and ends on a 16-byte boundary and
 // moves with one bulk copy.
-FPE_HD int fpe_block_stride(int nv) { return (nv * nv + 3) & ~3; }
-FPE_HD int fpe_fac_scratch_elems(int nv) {
-  const int p = fpe_fac_nvp(nv), t = p + 4;
-  const int aug = (nv * (nv + 1) + 3) & ~3;
-  return aug + p * p + p * t + 3 * p * t + 3 * p * t + 3 * p * p + 3 * p + (3 * p + 4);
+FPE_HD int fpe_block_stride(int b) { return (b * b + 3) & ~3; }
+FPE_HD int fpe_fac_scratch_elems(int b, int bw = 3) {
+  const int p = fpe_fac_nvp(b), t = p + 4;
+  const int aug = (b * (b + 1) + 3) & ~3;
+  return aug + p * p + p * t + bw * p * t + bw * p * t + bw * p * p + 3 * p + (3 * p + 4);
 }
 
 // Shared memory of the IC projection's ADMM (bytes): eigenvector matrices
@@ -206,11 +212,16 @@ FPE_HD FpeILayout fpe_ilayout(const FpeSolveDesc& d) {
   return L;
 }
 
-// Bytes of stage-system factor storage: one real block-banded LU (ns block
-// rows x 7 blocks of nv x nv) of element size esz, plus the same for the
-// complex system when requested (2 * esz per entry).
+// Bytes of stage-system factor storage: one real block-banded LU (ns m block
+// rows x 2 bw + 1 blocks of b x b) of element size esz, plus the same for the
+// complex system when requested (2 * esz per entry).  The kernel picks the
+// block split from the solve's actual nv; the size covers both splits.
 FPE_HD int64_t fpe_factor_bytes(const FpeSolveDesc& d, int esz, int with_complex) {
   int64_t blocks = int64_t(d.cap_dof_s) * 7 * fpe_block_stride(d.cap_dof_v);
+  if (d.blk_split == 2) {
+    const int64_t b2 = int64_t(d.cap_dof_s) * 2 * 15 * fpe_block_stride((d.cap_dof_v + 1) / 2);
+    if (b2 > blocks) blocks = b2;
+  }
   int64_t b = blocks * esz;
   if (with_complex) b += blocks * 2 * esz;
   return (b + 255) & ~int64_t(255);

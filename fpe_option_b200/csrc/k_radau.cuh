@@ -212,8 +212,12 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
   // factor scratch, 16-byte aligned (complex FP64 elements), in shared memory
   // when this solve's scratch fits in the launch's dynamic shared memory
   const int esz = int(sizeof(FT));
+  // stage-LU block structure: blocks of bsz = nv / m, bw off-diagonal blocks
+  const int msplit = fpe_blk_split(d.blk_split, nv), bsz = nv / msplit, bw = fpe_blk_bw(msplit);
+  const int nbr = ns * msplit;  // block rows
+  const int scr_elems = fpe_fac_scratch_elems(bsz, bw);
   const uintptr_t s_fac = (reinterpret_cast<uintptr_t>(fv + 5 * nv * 7) + 15) & ~uintptr_t(15);
-  const size_t fac_need = size_t(fpe_fac_scratch_elems(nv)) * esz * (direct ? 3 : 1) + (direct ? 16 : 0);
+  const size_t fac_need = size_t(scr_elems) * esz * (direct ? 3 : 1) + (direct ? 16 : 0);
   const bool fac_shared =
       !A.fac_global && (s_fac - reinterpret_cast<uintptr_t>(smem_raw)) + fac_need <= A.smem_bytes;
   void* sbig = fac_shared ? reinterpret_cast<void*>(s_fac) : reinterpret_cast<void*>(D + DL.fsc);
@@ -230,23 +234,25 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
   const OpFactors O{ns, nv, fs, fs + ns * 7, fs + 2 * ns * 7, fs + 3 * ns * 7,
                     fv, fv + nv * 7, fv + 2 * nv * 7, fv + 3 * nv * 7, fv + 4 * nv * 7};
   FT* fbase = reinterpret_cast<FT*>(A.farena + d.off_f);
-  const int bs = fpe_block_stride(nv);
-  const BlockLU<FT> LR{fbase, ns, nv, bs};
-  const BlockLU<Cx<FT>> LC{reinterpret_cast<Cx<FT>*>(fbase + size_t(ns) * 7 * bs), ns, nv, bs};
+  const int bs = fpe_block_stride(bsz);
+  const BlockLU<FT> LR{fbase, nbr, bsz, bs, bw, nv};
+  const BlockLU<Cx<FT>> LC{reinterpret_cast<Cx<FT>*>(fbase + size_t(nbr) * (2 * bw + 1) * bs), nbr, bsz, bs, bw, nv};
   // Staged sweeps when the stage buffers fit in the (shared) factorization
   // scratch, which is idle while the sweeps run.
   const long long fac_bytes = fac_shared ? (long long)fac_need : 0;
   // As many stage buffers (2 .. A.sweep_bufs) as the scratch holds.
-  const bool staged = fac_bytes >= stage_total_bytes(nv, esz, direct, 2);
+  const bool staged = fac_bytes >= stage_total_bytes(bsz, esz, direct, bw, 2);
   SolveStage SP;
   SP.nbuf = 2;
-  while (SP.nbuf < min(A.sweep_bufs, kMaxStageBufs) && fac_bytes >= stage_total_bytes(nv, esz, direct, SP.nbuf + 1))
+  while (SP.nbuf < min(A.sweep_bufs, kMaxStageBufs) &&
+         fac_bytes >= stage_total_bytes(bsz, esz, direct, bw, SP.nbuf + 1))
     ++SP.nbuf;
-  SP.slot_r = stage_slot_bytes(nv, esz);
-  SP.slot_c = stage_slot_bytes(nv, 2 * esz);
+  SP.slot_r = stage_slot_bytes(bsz, esz);
+  SP.slot_c = stage_slot_bytes(bsz, 2 * esz);
+  const int sbytes = stage_bytes(bsz, esz, direct, bw);
   for (int q = 0; q < kMaxStageBufs; ++q)
-    SP.buf[q] = reinterpret_cast<unsigned char*>(sbig) + size_t(min(q, SP.nbuf)) * stage_bytes(nv, esz, direct);
-  SP.ring = reinterpret_cast<void*>(SP.buf[0] + size_t(SP.nbuf) * stage_bytes(nv, esz, direct));
+    SP.buf[q] = reinterpret_cast<unsigned char*>(sbig) + size_t(min(q, SP.nbuf)) * sbytes;
+  SP.ring = reinterpret_cast<void*>(SP.buf[0] + size_t(SP.nbuf) * sbytes);
   SP.bar = S.pipe_bar;
   SP.err = &S.pipe_err;
   SP.wait_limit = d.stage_wait > 0 ? (long long)d.stage_wait : kBulkWaitLimit;
@@ -437,7 +443,7 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
       if (direct) blu_assemble<Cx<FT>>(O, LC, ALPH, BETA, h);
       FT* scr_r = reinterpret_cast<FT*>(sbig);
       Cx<FT>* scr_c = reinterpret_cast<Cx<FT>*>(
-          (reinterpret_cast<uintptr_t>(scr_r + fpe_fac_scratch_elems(nv)) + 15) & ~uintptr_t(15));
+          (reinterpret_cast<uintptr_t>(scr_r + scr_elems) + 15) & ~uintptr_t(15));
       const bool fac_ok = blu_factor_pair<FT>(LR, direct ? &LC : nullptr, scr_r, scr_c, t_fsub);
       t_factor += clock64() - t_f0;
       if (!fac_ok) {  // a zero or non-finite pivot: no step can use these factors

@@ -184,6 +184,12 @@ typedef struct FpeBatchOptions {
                             factor copies before the solve ends with FPE_STATUS_TIMEOUT
                             (<= 0 -> about one second); the FP64 retry always uses the
                             default.  A short limit exercises the failure path */
+    int32_t block_split; /* stage-LU block size: 0 auto (the tuned choice per grid size,
+                            else full nv x nv blocks when their factorization scratch fits
+                            in shared memory, half-width blocks when not), 1 nv x nv
+                            blocks, 2 (nv / 2) x (nv / 2) blocks (even nv) */
+    int32_t sweep_buffers; /* stage buffers of the staged block solves: 0 auto (the tuned
+                            choice, else 2), 2 .. 4 (as many as the shared scratch holds) */
 } FpeBatchOptions;
 
 /** Status codes written per strike slot of a batch. */

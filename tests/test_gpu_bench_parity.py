@@ -33,9 +33,9 @@ RTOL = 1e-6
 FLOOR = 1e-6 * 100.0
 
 
-def _opts(fpe, precision):
+def _opts(fpe, precision, **kw):
     return fpe.BatchOptions(disc=1, precision=precision, rtol=RTOL, atol=RTOL * 1e-2, complex_solve=2,
-                            radau_constants=2)
+                            radau_constants=2, **kw)
 
 
 def _oracle(oracle, P, I):
@@ -47,26 +47,25 @@ def _rel(p, ref):
     return np.abs(p - ref) / np.maximum(np.abs(ref), FLOOR)
 
 
-def bench_class_sample(I, per_class=2):
-    """The first `per_class` contracts of each (n_s, n_v) class, in batch order."""
-    idx = []
-    for ns in (32, 48, 64):
-        for nv in (16, 24, 32):
-            idx += list(np.flatnonzero((I[:, 0] == ns) & (I[:, 1] == nv))[:per_class])
-    return np.array(sorted(idx))
+_BATCH_REF = {}
 
 
-def test_batched_workload_vs_oracle(engine, oracle):
+@pytest.mark.parametrize("block_split", [1, 2])
+def test_batched_workload_vs_oracle(engine, oracle, block_split):
+    """Both stage-LU block structures (nv x nv blocks, and half-width blocks with
+    seven off-diagonal blocks a side) against the same oracle prices."""
     import bench
 
     fpe = engine
     P, I = bench.make_batch(bench.N_CONTRACTS, 0)
-    idx = bench_class_sample(I)
+    idx = bench.class_sample(I)
     assert len(idx) == 18
     Ps, Is = P[idx], I[idx]
-    ref = _oracle(oracle, Ps, Is)
-    p64, s64 = fpe.price_batch(Ps, Is, _opts(fpe, 0))
-    p32, s32 = fpe.price_batch(Ps, Is, _opts(fpe, 1))
+    if "ref" not in _BATCH_REF:
+        _BATCH_REF["ref"] = _oracle(oracle, Ps, Is)
+    ref = _BATCH_REF["ref"]
+    p64, s64 = fpe.price_batch(Ps, Is, _opts(fpe, 0, block_split=block_split))
+    p32, s32 = fpe.price_batch(Ps, Is, _opts(fpe, 1, block_split=block_split))
     assert (s64 == 0).all() and (s32 == 0).all()
     assert _rel(p64, ref).max() < 1e-7, _rel(p64, ref)
     assert _rel(p32, ref).max() < 1e-4, _rel(p32, ref)

@@ -98,9 +98,10 @@ def test_noalloc_default_domain_and_caller_stream(engine):
 
 
 def test_noalloc_global_factor_scratch(engine):
-    """48 v-dofs in mixed precision: the stage-factorization scratch does not fit
-    in shared memory and lives in the static array (the kernel's global branch)."""
-    opts = engine.BatchOptions(disc=1, precision=1, rtol=1e-6, atol=1e-8)
+    """48 v-dofs in mixed precision with full-width (48 x 48) stage-LU blocks:
+    the factorization scratch does not fit in shared memory and lives in the
+    static array (the kernel's global branch)."""
+    opts = engine.BatchOptions(disc=1, precision=1, rtol=1e-6, atol=1e-8, block_split=1)
     ref, outs = _both(engine, [60.0], 8, 0.0, 16, opts, n_v=48)
     for got in outs:
         np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-14)
