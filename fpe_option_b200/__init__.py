@@ -130,6 +130,9 @@ def _require():
     L = _lib.load()
     if not L.fpe_device_available():
         raise RuntimeError("FPE GPU engine not available (no usable CUDA device)")
+    from . import autotune
+
+    autotune.load_default()  # the tuned solve shapes measured on a B200, once
     return L
 
 
@@ -452,6 +455,7 @@ class BatchOptions:
     stage_wait_cycles: int = 0  # <= 0: ~1 s bounded wait per staged sweep stage
     block_split: int = 0     # stage-LU blocks: 0 auto, 1 nv x nv, 2 (nv/2) x (nv/2)
     sweep_buffers: int = 0   # staged-sweep buffers: 0 auto, 2..4
+    knock_in_tol_scale: float = 0.0  # knock-in solve pairs: rtol/atol factor (<= 0: 1 disc 0, 0.01 disc 1)
 
     def to_c(self) -> _lib.FpeBatchOptions:
         o = _lib.FpeBatchOptions()
@@ -467,6 +471,7 @@ class BatchOptions:
         o.max_steps, o.fp64_retry = self.max_steps, self.fp64_retry
         o.stage_wait_cycles = self.stage_wait_cycles
         o.block_split, o.sweep_buffers = self.block_split, self.sweep_buffers
+        o.knock_in_tol_scale = self.knock_in_tol_scale
         return o
 
 

@@ -56,7 +56,8 @@ class FpeBatchOptions(C.Structure):
                 ("greeks", i32), ("rel_s", d), ("rel_v", d), ("complex_solve", i32),
                 ("radau_constants", i32), ("max_step", d), ("first_step", d),
                 ("price_rule", i32), ("max_steps", i32), ("fp64_retry", i32),
-                ("stage_wait_cycles", i64), ("block_split", i32), ("sweep_buffers", i32)]
+                ("stage_wait_cycles", i64), ("block_split", i32), ("sweep_buffers", i32),
+                ("knock_in_tol_scale", d)]
 
 
 # Every symbol declared in include/*.h.
@@ -68,7 +69,8 @@ EXPORTED = [
     "fpe_compute_free_oneshot", "fpe_plan_create", "fpe_plan_run", "fpe_plan_results",
     "fpe_plan_stats", "fpe_plan_sizes", "fpe_plan_destroy", "fpe_price_batch",
     "fpe_compute_create_ex", "fpe_compute_basis_csr", "fpe_device_available",
-    "fpe_plan_kernel_times", "fpe_plan_retried", "fpe_plan_solve_info", "fpe_price_noalloc", "fpe_heston_cf_batch", "fpe_heston_cf_price",
+    "fpe_plan_kernel_times", "fpe_plan_retried", "fpe_plan_solve_info", "fpe_tune_set", "fpe_tune_get",
+    "fpe_tune_clear", "fpe_price_noalloc", "fpe_heston_cf_batch", "fpe_heston_cf_price",
     "fpe_pdf_interpolate",
     # include/fpe_surrogate.h
     "fpe_mlp_create", "fpe_mlp_destroy", "fpe_mlp_layout", "fpe_mlp_get_params",
@@ -127,6 +129,12 @@ def load():
     L.fpe_plan_retried.argtypes = [cp]
     L.fpe_plan_solve_info.restype = i32
     L.fpe_plan_solve_info.argtypes = [cp, ip]
+    L.fpe_tune_set.restype = i32
+    L.fpe_tune_set.argtypes = [i32] * 7
+    L.fpe_tune_get.restype = i32
+    L.fpe_tune_get.argtypes = [i32] * 5 + [ip, ip]
+    L.fpe_tune_clear.restype = None
+    L.fpe_tune_clear.argtypes = []
     L.fpe_plan_destroy.argtypes = [cp]
     L.fpe_price_batch.restype = i32
     L.fpe_price_batch.argtypes = [C.POINTER(FpeContract), i32, C.POINTER(FpeBatchOptions),

@@ -25,6 +25,12 @@
 #include "dev_common.cuh"
 #include "bulk_pipe.cuh"
 
+// The pivot-block inverse used by the factorization (fac_gj: registers for FP32
+// blocks where it can; fac_gj_warp: shared-memory rows).
+#ifndef FPE_GJ
+#define FPE_GJ fac_gj
+#endif
+
 namespace fpe {
 
 template <typename T>
@@ -232,12 +238,13 @@ __device__ __forceinline__ double fmag(Cx<T> a) {
 //   EbT  bw x nvp x ldt   E_{i+1+r, i}, transposed
 //   LbT  bw x nvp x ldt   L_{i+1+r, i} = E P^-1, transposed (left operand of the Schur update)
 //   Ub   bw x nvp x nvp   U_{i, i+1+c}, row-major
+//   pbuf 2 x nvp          the published pivot row of the register Gauss-Jordan
 //   pinv nvp (inverse pivot of each column), then the pivot rows prow_of and
 //   their columns q_of (int)
 // --------------------------------------------------------------------------
 template <typename ET>
 struct FacScratch {
-  ET *aug, *Pi, *PiT, *EbT, *LbT, *Ub;
+  ET *aug, *Pi, *PiT, *EbT, *LbT, *Ub, *pbuf;
   ET* pinv;      // inverse pivot value of each column
   int* prow_of;  // pivot row of each column
   int* q_of;     // column whose pivot row is r
@@ -256,7 +263,8 @@ struct FacScratch {
     EbT = PiT + p * t;
     LbT = EbT + bw * p * t;
     Ub = LbT + bw * p * t;
-    pinv = Ub + bw * p * p;
+    pbuf = Ub + bw * p * p;
+    pinv = pbuf + 2 * p;
     prow_of = reinterpret_cast<int*>(pinv + p);
     q_of = prow_of + p;
   }
@@ -506,6 +514,95 @@ __device__ bool fac_gj_warp(FacScratch<ET>& S) {
   return ok;
 }
 
+// The same Gauss-Jordan inversion with each lane's row in registers (FP32
+// blocks of NV <= 32 columns): lane r keeps row r for the whole inversion, and
+// the pivot lane publishes its row each step through one of two alternating
+// shared rows (the next step writes the other, so one __syncwarp per step
+// orders a publication before its reads and after the previous-but-one
+// step's reads).  The row rotates left by one column per step, so the current
+// column is always element 0 and the loop body is one compiled step; after NV
+// steps the columns are back in order.  The pivot choice, the arithmetic of
+// each element and the bookkeeping are those of fac_gj_warp.
+template <typename ET, int NV>
+__device__ __noinline__ bool fac_gj_warp_reg(FacScratch<ET>& S) {
+  static_assert(NV <= 32 && NV % 4 == 0, "register rows of up to 32 columns, 16-byte chunks");
+  const int lane = threadIdx.x & 31, w1 = S.w1;
+  const bool own = lane < NV;
+  ET row[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) row[l] = own ? S.aug[lane * w1 + l] : fzero(ET());
+  bool used = false, ok = true;
+#pragma unroll 1
+  for (int c = 0; c < NV; ++c) {
+    const unsigned k = (own && !used) ? pivot_key(pmag(row[0]), lane) : 0u;
+    const unsigned kmax = __reduce_max_sync(0xffffffffu, k);
+    const int p = min(127 - int(kmax & 127u), NV - 1);  // an unused row always has a nonzero key
+    ET* pb = S.pbuf + (c & 1) * NV;
+    if (lane == p) {
+#pragma unroll
+      for (int l = 0; l < NV; ++l) pb[l] = row[l];
+    }
+    __syncwarp();
+    const ET pv = pb[0];
+    const float pm = pmag(pv);
+    ok &= (pm > 0.f) && (pm < CUDART_INF_F);
+    const ET inv = finv(pv);
+    if (lane == 0) {
+      S.prow_of[c] = p;
+      S.q_of[p] = c;
+      S.pinv[c] = inv;
+    }
+    if (lane == p) {
+      used = true;
+      row[0] = fone(ET());
+    } else if (own) {
+      const ET f = fmul(row[0], inv);
+#pragma unroll
+      for (int l0 = 0; l0 < NV; l0 += 4) {
+        ET q[4];
+        vld<4>(pb + l0, q);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (l0 + j > 0) row[l0 + j] = fsub(row[l0 + j], fmul(f, q[j]));
+      }
+      row[0] = fsub(fzero(ET()), f);
+    }
+    const ET t0 = row[0];
+#pragma unroll
+    for (int l = 0; l + 1 < NV; ++l) row[l] = row[l + 1];
+    row[NV - 1] = t0;
+  }
+  if (own) {
+#pragma unroll
+    for (int l = 0; l < NV; ++l) S.aug[lane * w1 + l] = row[l];
+  }
+  return ok;
+}
+
+template <typename ET>
+struct IsF32Elem { static constexpr bool v = false; };
+template <>
+struct IsF32Elem<float> { static constexpr bool v = true; };
+template <>
+struct IsF32Elem<Cx<float>> { static constexpr bool v = true; };
+
+// The pivot-block inverse: rows in registers for FP32 blocks of 8 to 32
+// columns (multiples of 4), rows in shared memory otherwise.
+template <typename ET>
+__device__ bool fac_gj(FacScratch<ET>& S) {
+  if constexpr (IsF32Elem<ET>::v) {
+    switch (S.nv) {
+      case 8: return fac_gj_warp_reg<ET, 8>(S);
+      case 12: return fac_gj_warp_reg<ET, 12>(S);
+      case 16: return fac_gj_warp_reg<ET, 16>(S);
+      case 24: return fac_gj_warp_reg<ET, 24>(S);
+      case 32: return fac_gj_warp_reg<ET, 32>(S);
+      default: break;
+    }
+  }
+  return fac_gj_warp<ET>(S);
+}
+
 // P^-1 (row k = row p_k of the array scaled by 1 / a_{p_k k}, columns
 // un-permuted) into Pi, PiT and the factor storage.
 template <typename ET>
@@ -631,7 +728,7 @@ __device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int n
 // fpe_fac_scratch_elems(b, bw) elements each.
 template <typename FT>
 __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC, FT* scr_r,
-                                Cx<FT>* scr_c, long long (&tcyc)[3]) {
+                                Cx<FT>* scr_c, long long (&tcyc)[4]) {
   const int ns = LR.nb, bw = LR.bw;  // block rows, off-diagonal blocks
   FacScratch<FT> SR;
   SR.init(scr_r, LR.b, bw);
@@ -651,13 +748,14 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
     fac_stage<FT>(LR, SR, 0, min(bw, ns - 1));
     if (LC) fac_stage<Cx<FT>>(*LC, SC, 0, min(bw, ns - 1));
     __syncthreads();
-    if (warp == 0) ok &= fac_gj_warp<FT>(SR);
-    else if (warp == 1 && LC) ok &= fac_gj_warp<Cx<FT>>(SC);
+    if (warp == 0) ok &= FPE_GJ<FT>(SR);
+    else if (warp == 1 && LC) ok &= FPE_GJ<Cx<FT>>(SC);
     __syncthreads();
     tcyc[0] += clock64() - t0;
   }
   for (int i = 0; i < ns; ++i) {
     const int nr = min(i + bw, ns - 1) - i;
+    const long long t1 = clock64();
     if (i > 0) {  // U and E blocks of row i (its pivot block is already inverted)
       fac_stage<FT>(LR, SR, i, nr, false, true);
       if (LC) fac_stage<Cx<FT>>(*LC, SC, i, nr, false, true);
@@ -666,6 +764,7 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
     fac_extract<FT>(LR, SR, i);
     if (LC) fac_extract<Cx<FT>>(*LC, SC, i);
     __syncthreads();
+    tcyc[3] += clock64() - t1;
     if (nr > 0) {
       const long long t2 = clock64();
       fac_lw<FT>(LR, SR, i, nr);
@@ -687,9 +786,9 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
       tcyc[1] += t3 - t2;
       if (split) {
         if (warp == 0) {
-          ok &= fac_gj_warp<FT>(SR);
+          ok &= FPE_GJ<FT>(SR);
         } else if (warp == 1) {
-          if (LC) ok &= fac_gj_warp<Cx<FT>>(SC);
+          if (LC) ok &= FPE_GJ<Cx<FT>>(SC);
         } else {
           const int lt = threadIdx.x - 64, nt = blockDim.x - 64;
           fac_update<FT, false>(LR, SR, i, nr, 1, nr * nr, lt, nt);
@@ -701,8 +800,8 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
         fac_update<FT, false>(LR, SR, i, nr, 1, nr * nr, threadIdx.x, blockDim.x);
         if (LC) fac_update<Cx<FT>, false>(*LC, SC, i, nr, 1, nr * nr, threadIdx.x, blockDim.x);
         __syncthreads();
-        if (warp == 0) ok &= fac_gj_warp<FT>(SR);
-        else if (warp == 1 && LC) ok &= fac_gj_warp<Cx<FT>>(SC);
+        if (warp == 0) ok &= FPE_GJ<FT>(SR);
+        else if (warp == 1 && LC) ok &= FPE_GJ<Cx<FT>>(SC);
       }
       __syncthreads();
       tcyc[0] += clock64() - t3;
@@ -1119,6 +1218,17 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
         }
       }
       RT ar = RT(0), ai = RT(0), zr = RT(0), zi = RT(0);
+      // the row's right-hand side (forward) or z (backward), loaded before the products
+      double cre = 0.0, cim = 0.0;
+      if (is_c && cg == 0) {
+        if (!fwd) {
+          cre = S.zc_re[i * nv + cj];
+          cim = S.zc_im[i * nv + cj];
+        } else if (i < ns) {
+          cre = S.xc_re[i * nv + cj];
+          cim = S.xc_im[i * nv + cj];
+        }
+      }
       if (is_c) {
         const unsigned char* cb = buf + ng * P.slot_r;
         for (int g = cg; g < ng; g += Gc) {
@@ -1149,15 +1259,15 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
       if (is_c && cg == 0) {
         if (fwd) {
           if (i < ns) {
-            ring_c_re[(i & rmask) * nv + cj] = RT(S.xc_re[i * nv + cj] - double(ar));
-            ring_c_im[(i & rmask) * nv + cj] = RT(S.xc_im[i * nv + cj] - double(ai));
+            ring_c_re[(i & rmask) * nv + cj] = RT(cre - double(ar));
+            ring_c_im[(i & rmask) * nv + cj] = RT(cim - double(ai));
           }
           if (i >= 1) {
             S.zc_re[(i - 1) * nv + cj] = double(zr);
             S.zc_im[(i - 1) * nv + cj] = double(zi);
           }
         } else {
-          const double xr = S.zc_re[i * nv + cj] - double(ar), xi = S.zc_im[i * nv + cj] - double(ai);
+          const double xr = cre - double(ar), xi = cim - double(ai);
           ring_c_re[(i & rmask) * nv + cj] = RT(xr);
           ring_c_im[(i & rmask) * nv + cj] = RT(xi);
           S.xc_re[i * nv + cj] = xr;

@@ -15,7 +15,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "../../include/fpe_engine.h"
@@ -35,6 +37,9 @@ static_assert(FPE_SOLVE_INFO_WORDS == FPE_INFO_COUNT, "per-solve info words of t
 #ifndef FPE_SWEEP_BUFS
 #define FPE_SWEEP_BUFS 2
 #endif
+
+// Reads a table of tuned solve shapes (the autotuner's section below).
+static void tune_load_file(const char* path);
 
 namespace {
 
@@ -65,6 +70,7 @@ Context& ctx() {
     if (cudaGetDevice(&c.device) != cudaSuccess) return;
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return;
     cudaDeviceGetAttribute(&c.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device);
+    tune_load_file(std::getenv("FPE_TUNE_TABLE"));
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, c.device) == cudaSuccess) {
       uint64_t thr = UINT64_MAX;
@@ -125,6 +131,7 @@ struct Opts {
   int fp64_retry = 1;                       // re-solve failed mixed solves with FP64 factors
   long long stage_wait = 0;                 // <= 0: about one second
   int block_split = 0;                      // 0 auto, 1 nv x nv blocks, 2 half-width blocks
+  double ki_scale = 1.0;                    // tolerance factor of a knock-in's two solves
   int sweep_buffers = 0;                    // 0 auto, 2 .. 4
 };
 
@@ -157,6 +164,8 @@ Opts opts_from(const FpeBatchOptions* o, int default_num_insert) {
   r.fp64_retry = o->fp64_retry < 0 ? 0 : 1;
   r.stage_wait = o->stage_wait_cycles > 0 ? (long long)o->stage_wait_cycles : 0;
   r.block_split = (o->block_split == 1 || o->block_split == 2) ? o->block_split : 0;
+  r.ki_scale = (o->knock_in_tol_scale > 0.0 && std::isfinite(o->knock_in_tol_scale)) ? o->knock_in_tol_scale
+                                                                                    : (o->disc == 1 ? 0.01 : 1.0);
   r.sweep_buffers = (o->sweep_buffers >= 2 && o->sweep_buffers <= 4) ? o->sweep_buffers : 0;
   return r;
 }
@@ -226,6 +235,17 @@ FpeSolveDesc make_desc(const Pricing& p, int solve_type, double barrier, const O
   return d;
 }
 
+// The options of a knock-in's two solves (in-out parity, reference
+// src/server/pricer.mojo:87-120): the tolerances scaled by ki_scale, since
+// the difference of the vanilla and knock-out prices amplifies their
+// relative errors by vanilla / knock-in.
+Opts knock_in_opts(const Opts& o) {
+  Opts r = o;
+  r.rtol *= o.ki_scale;
+  r.atol *= o.ki_scale;
+  return r;
+}
+
 }  // namespace
 
 // --------------------------------------------------------------------------
@@ -277,12 +297,63 @@ static size_t radau_smem_need(const FpeSolveDesc& d, int esz, int cplx, size_t* 
   return *base + el * esz + (cplx ? el * 2 * esz + 16 : 0);
 }
 
-// The stage-LU block split of a solve: the caller's choice, else full nv x nv
-// blocks when their factorization scratch fits in shared memory and
-// half-width blocks when it does not (nv = 48 in mixed precision, for one).
-static void resolve_block_split(FpeSolveDesc& d, const Opts& o, int esz, size_t optin) {
+// --------------------------------------------------------------------------
+// Tuned solve shapes.  For a grid class (discretization, n_s, n_v knot
+// inputs, factor precision, complex stage mode) the autotuner
+// (fpe_option_b200/autotune.py) times the candidate shapes on the device and
+// installs the fastest here; a plan's solves look their class up.  The table
+// can also be read from a text file named by FPE_TUNE_TABLE at start-up (one
+// class per line: disc n_s n_v precision complex_solve block_split
+// sweep_buffers).
+// --------------------------------------------------------------------------
+struct TuneShape {
+  int block_split = 0, sweep_buffers = 0;
+};
+using TuneKey = std::tuple<int, int, int, int, int>;  // disc, n_s, n_v, precision, complex mode
+
+static std::mutex& tune_mu() {
+  static std::mutex m;
+  return m;
+}
+static std::map<TuneKey, TuneShape>& tune_table() {
+  static std::map<TuneKey, TuneShape> t;
+  return t;
+}
+static bool tune_find(const TuneKey& k, TuneShape* out) {
+  std::lock_guard<std::mutex> lock(tune_mu());
+  auto it = tune_table().find(k);
+  if (it == tune_table().end()) return false;
+  *out = it->second;
+  return true;
+}
+static void tune_load_file(const char* path) {
+  FILE* f = path ? std::fopen(path, "r") : nullptr;
+  if (!f) return;
+  char line[256];
+  std::lock_guard<std::mutex> lock(tune_mu());
+  while (std::fgets(line, sizeof(line), f)) {
+    int v[7];
+    if (line[0] == '#') continue;
+    if (std::sscanf(line, "%d %d %d %d %d %d %d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6]) != 7) continue;
+    tune_table()[TuneKey{v[0], v[1], v[2], v[3], v[4]}] = TuneShape{v[5], v[6]};
+  }
+  std::fclose(f);
+}
+
+// The shape of a solve: the caller's explicit choices, else the tuned shape of
+// its grid class, else full nv x nv blocks when their factorization scratch
+// fits in shared memory and half-width blocks when it does not (nv = 48 in
+// mixed precision, for one), with the launch's default stage buffers.
+static void resolve_solve_shape(FpeSolveDesc& d, const Opts& o, int esz, size_t optin) {
+  TuneShape t;
+  const bool tuned = tune_find(TuneKey{o.disc, d.n_s, d.n_v, esz == 8 ? 0 : 1, o.complex_mode}, &t);
+  d.sweep_bufs = o.sweep_buffers ? o.sweep_buffers : (tuned ? t.sweep_buffers : 0);
   if (o.block_split) {
     d.blk_split = o.block_split;
+    return;
+  }
+  if (tuned && t.block_split) {
+    d.blk_split = t.block_split;
     return;
   }
   d.blk_split = 1;
@@ -296,7 +367,7 @@ static int plan_layout(FpePlan* P, int esz) {
   const size_t optin = size_t(ctx().smem_optin > 0 ? ctx().smem_optin : 232448);
   const int cplx = P->o.complex_mode;
   for (auto& d : P->descs) {
-    resolve_block_split(d, P->o, esz, optin);
+    resolve_solve_shape(d, P->o, esz, optin);
     d.off_d = od;
     d.off_i = oi;
     d.off_f = of;
@@ -445,10 +516,11 @@ static FpePlan* plan_build(const FpeContract* c, int n, const Opts& o, bool save
     if (ot == 0 || ot == 1 || ot == 4 || ot == 5) {
       const bool call = ot % 2 == 0, down = ot <= 1;
       int out_type = (down ? 2 : 6) + (call ? 0 : 1);
+      const Opts oki = knock_in_opts(o);
       p.solve_a = int(P->descs.size());
-      P->descs.push_back(make_desc(p, call ? 8 : 9, 0.0, o));
+      P->descs.push_back(make_desc(p, call ? 8 : 9, 0.0, oki));
       p.solve_b = int(P->descs.size());
-      P->descs.push_back(make_desc(p, out_type, p.barrier, o));
+      P->descs.push_back(make_desc(p, out_type, p.barrier, oki));
     } else {
       p.solve_a = int(P->descs.size());
       P->descs.push_back(make_desc(p, ot, p.barrier, o));
@@ -848,6 +920,31 @@ int32_t fpe_plan_results(FpePlan* P, double* prices, double* delta, double* gamm
 }
 
 int32_t fpe_plan_retried(FpePlan* P) { return P ? P->n_retried : -1; }
+
+int32_t fpe_tune_set(int32_t disc, int32_t n_s, int32_t n_v, int32_t precision, int32_t complex_solve,
+                     int32_t block_split, int32_t sweep_buffers) {
+  if (block_split < 0 || block_split > 2 || (sweep_buffers != 0 && (sweep_buffers < 2 || sweep_buffers > 4)))
+    return -1;
+  const int cm = complex_solve == 2 ? 1 : complex_solve == 1 ? 0 : (disc == 1 ? 1 : 0);
+  std::lock_guard<std::mutex> lock(tune_mu());
+  tune_table()[TuneKey{disc, n_s, n_v, precision ? 1 : 0, cm}] = TuneShape{block_split, sweep_buffers};
+  return 0;
+}
+
+int32_t fpe_tune_get(int32_t disc, int32_t n_s, int32_t n_v, int32_t precision, int32_t complex_solve,
+                     int32_t* block_split, int32_t* sweep_buffers) {
+  const int cm = complex_solve == 2 ? 1 : complex_solve == 1 ? 0 : (disc == 1 ? 1 : 0);
+  TuneShape t;
+  if (!tune_find(TuneKey{disc, n_s, n_v, precision ? 1 : 0, cm}, &t)) return 0;
+  if (block_split) *block_split = t.block_split;
+  if (sweep_buffers) *sweep_buffers = t.sweep_buffers;
+  return 1;
+}
+
+void fpe_tune_clear(void) {
+  std::lock_guard<std::mutex> lock(tune_mu());
+  tune_table().clear();
+}
 
 int32_t fpe_plan_solve_info(FpePlan* P, int32_t* out) {
   if (!P || !out) return -1;
@@ -1262,8 +1359,9 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
   const int ot = p.type;
   if (ot == 0 || ot == 1 || ot == 4 || ot == 5) {
     const bool call = ot % 2 == 0, down = ot <= 1;
-    d[0] = make_desc(p, call ? 8 : 9, 0.0, o);
-    d[1] = make_desc(p, (down ? 2 : 6) + (call ? 0 : 1), p.barrier, o);
+    const Opts oki = knock_in_opts(o);
+    d[0] = make_desc(p, call ? 8 : 9, 0.0, oki);
+    d[1] = make_desc(p, (down ? 2 : 6) + (call ? 0 : 1), p.barrier, oki);
     nsolve = 2;
   } else {
     d[0] = make_desc(p, ot, p.barrier, o);
@@ -1284,7 +1382,7 @@ extern "C" int32_t fpe_price_noalloc(const FpeContract* contract, const FpeBatch
   int64_t od = 0, oi = 0, of = 0;
   size_t smem_max = 0, smem_base = 0, ic = 0;
   for (int k = 0; k < nsolve; ++k) {
-    resolve_block_split(d[k], o, esz, size_t(ND->smem_optin));
+    resolve_solve_shape(d[k], o, esz, size_t(ND->smem_optin));
     d[k].strike_off = k * nk;
     d[k].off_d = od;
     d[k].off_i = oi;

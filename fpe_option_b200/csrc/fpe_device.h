@@ -44,6 +44,8 @@ enum FpeInfo {
   // (kilocycles): the real pivot inverse (warp 0), the complex one (warp 1)
   // and the other Schur updates (warp 2)
   FPE_INFO_T_GJ_REAL, FPE_INFO_T_GJ_CPLX, FPE_INFO_T_SCHUR,
+  FPE_INFO_T_FASM,    // inside T_FACTOR: stage-matrix assembly (kilocycles)
+  FPE_INFO_T_FSTAGE,  // inside T_FACTOR: staging of each block row and the pivot-inverse extraction
   FPE_INFO_COUNT = 32
 };
 
@@ -68,6 +70,8 @@ struct FpeSolveDesc {
   int32_t traj_cap;      // max saved states
   int32_t max_steps;     // accepted-step cap (radau.mojo:257-263: 100000)
   int32_t blk_split;     // stage-LU block size nv / blk_split (1 or 2; see fpe_blk_split)
+  int32_t sweep_bufs;    // stage buffers of the staged sweeps (2 .. 4; 0: the launch's default)
+  int32_t pad1;
   int64_t stage_wait;    // SM cycles a staged sweep waits for its copies (<= 0: ~1 s)
   // capacities
   int32_t cap_knot_s, cap_knot_v, cap_grid_s, cap_grid_v, cap_q_s, cap_q_v;
@@ -125,7 +129,8 @@ FPE_HD int fpe_blk_bw(int m) { return 4 * m - 1; }
 // and bw off-diagonal blocks: the pivot block's Gauss-Jordan array
 // b x (b + 1), then blocks padded to p = b rounded up to 4 (row-major p x p,
 // transposed p x (p + 4)): P^-1 both ways, bw transposed E and L blocks, bw U
-// blocks, and the pivot bookkeeping (with room to spare).
+// blocks, two pivot-row buffers of p, and the pivot bookkeeping (with room to
+// spare).
 FPE_HD int fpe_fac_nvp(int nv) { return (nv + 3) & ~3; }
 // Element stride between the b x b blocks of a stored stage factor: b^2
 // rounded up to 4, so every block starts and ends on a 16-byte boundary and
@@ -134,7 +139,7 @@ FPE_HD int fpe_block_stride(int b) { return (b * b + 3) & ~3; }
 FPE_HD int fpe_fac_scratch_elems(int b, int bw = 3) {
   const int p = fpe_fac_nvp(b), t = p + 4;
   const int aug = (b * (b + 1) + 3) & ~3;
-  return aug + p * p + p * t + bw * p * t + bw * p * t + bw * p * p + 3 * p + (3 * p + 4);
+  return aug + p * p + p * t + bw * p * t + bw * p * t + bw * p * p + 2 * p + 3 * p + (3 * p + 4);
 }
 
 // Shared memory of the IC projection's ADMM (bytes): eigenvector matrices

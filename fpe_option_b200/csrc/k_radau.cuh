@@ -240,11 +240,13 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
   // Staged sweeps when the stage buffers fit in the (shared) factorization
   // scratch, which is idle while the sweeps run.
   const long long fac_bytes = fac_shared ? (long long)fac_need : 0;
-  // As many stage buffers (2 .. A.sweep_bufs) as the scratch holds.
+  // As many stage buffers (2 .. the solve's or the launch's choice) as the
+  // scratch holds.
   const bool staged = fac_bytes >= stage_total_bytes(bsz, esz, direct, bw, 2);
+  const int want_bufs = d.sweep_bufs > 0 ? d.sweep_bufs : A.sweep_bufs;
   SolveStage SP;
   SP.nbuf = 2;
-  while (SP.nbuf < min(A.sweep_bufs, kMaxStageBufs) &&
+  while (SP.nbuf < min(want_bufs, kMaxStageBufs) &&
          fac_bytes >= stage_total_bytes(bsz, esz, direct, bw, SP.nbuf + 1))
     ++SP.nbuf;
   SP.slot_r = stage_slot_bytes(bsz, esz);
@@ -283,7 +285,8 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
   // phase timers (SM clock cycles, thread 0 reports)
   const long long t_kernel0 = clock64();
   long long t_factor = 0, t_solve = 0, t_kron = 0;
-  long long t_fsub[3] = {0, 0, 0};  // factorization: overlapped phase, products, own role's work
+  long long t_fsub[4] = {0, 0, 0, 0};  // factorization: overlapped phase, products, own role's work, staging
+  long long t_fasm = 0;                // stage-matrix assembly
 #define KRON(...)                          \
   do {                                     \
     const long long t_k0 = clock64();      \
@@ -441,6 +444,7 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
       const long long t_f0 = clock64();
       blu_assemble<FT>(O, LR, U1, 0.0, h);
       if (direct) blu_assemble<Cx<FT>>(O, LC, ALPH, BETA, h);
+      t_fasm += clock64() - t_f0;
       FT* scr_r = reinterpret_cast<FT*>(sbig);
       Cx<FT>* scr_c = reinterpret_cast<Cx<FT>*>(
           (reinterpret_cast<uintptr_t>(scr_r + scr_elems) + 15) & ~uintptr_t(15));
@@ -825,6 +829,8 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
     info[FPE_INFO_T_FGEMM] = int(t_fsub[1] >> 10);
     info[FPE_INFO_T_SWAIT] = int(t_swait >> 10);
     info[FPE_INFO_T_GJ_REAL] = int(t_fsub[2] >> 10);
+    info[FPE_INFO_T_FASM] = int(t_fasm >> 10);
+    info[FPE_INFO_T_FSTAGE] = int(t_fsub[3] >> 10);
   }
   if (threadIdx.x == 32) info[FPE_INFO_T_GJ_CPLX] = int(t_fsub[2] >> 10);
   if (threadIdx.x == 64) info[FPE_INFO_T_SCHUR] = int(t_fsub[2] >> 10);

@@ -190,6 +190,12 @@ typedef struct FpeBatchOptions {
                             blocks, 2 (nv / 2) x (nv / 2) blocks (even nv) */
     int32_t sweep_buffers; /* stage buffers of the staged block solves: 0 auto (the tuned
                             choice, else 2), 2 .. 4 (as many as the shared scratch holds) */
+    double knock_in_tol_scale; /* rtol and atol of both solves of a knock-in (in-out
+                            parity) are multiplied by this: the price is the difference
+                            of two larger prices, so their relative errors are amplified
+                            by vanilla / knock-in.  <= 0 -> 1 on the reference
+                            discretization (the reference Pricer), 0.01 on the config
+                            discretization */
 } FpeBatchOptions;
 
 /** Status codes written per strike slot of a batch. */
@@ -237,6 +243,22 @@ extern int32_t fpe_plan_sizes(FpePlan* plan, int32_t* n_results, int32_t* n_solv
 /** Solves of the last fpe_plan_results call that were solved again with FP64
  *  factors after a mixed-precision failure (opt->fp64_retry), or < 0. */
 extern int32_t fpe_plan_retried(FpePlan* plan);
+/** Tuned solve shape of a grid class, used by plans whose block_split /
+ *  sweep_buffers options are 0 (auto).  No reference counterpart: the
+ *  autotuner (fpe_option_b200/autotune.py) times the candidate shapes of each
+ *  class on the device and installs the fastest here.  A class is (disc, n_s,
+ *  n_v, precision, complex_solve) as in FpeContract / FpeBatchOptions;
+ *  block_split 0 keeps the shared-memory fit rule.  The table can also be
+ *  loaded at start-up from the text file named by the environment variable
+ *  FPE_TUNE_TABLE (lines: disc n_s n_v precision complex_solve block_split
+ *  sweep_buffers).  fpe_tune_set returns 0 or < 0 on a bad shape;
+ *  fpe_tune_get returns 1 and fills the shape when the class is tuned, else 0. */
+extern int32_t fpe_tune_set(int32_t disc, int32_t n_s, int32_t n_v, int32_t precision, int32_t complex_solve,
+                            int32_t block_split, int32_t sweep_buffers);
+extern int32_t fpe_tune_get(int32_t disc, int32_t n_s, int32_t n_v, int32_t precision, int32_t complex_solve,
+                            int32_t* block_split, int32_t* sweep_buffers);
+extern void fpe_tune_clear(void);
+
 /** Number of words per solve in fpe_plan_solve_info. */
 #define FPE_SOLVE_INFO_WORDS 32
 /** Per-solve counters of the plan's last run, FPE_SOLVE_INFO_WORDS words per
@@ -247,7 +269,9 @@ extern int32_t fpe_plan_retried(FpePlan* plan);
  *  and in total, 22-23 the factorization's pivot inverses and block
  *  products, 24 the sweeps' waits for their factor copies, 25-27 the
  *  overlapped factorization phase's own work of the real pivot inverse, the
- *  complex pivot inverse and the other Schur updates.  out holds
+ *  complex pivot inverse and the other Schur updates, 28 the stage
+ *  matrices' assembly, 29 the block rows' staging and pivot-inverse
+ *  extraction.  out holds
  *  n_solves * FPE_SOLVE_INFO_WORDS words.  Returns n_solves, < 0 on error. */
 extern int32_t fpe_plan_solve_info(FpePlan* plan, int32_t* out);
 extern void fpe_plan_destroy(FpePlan* plan);
