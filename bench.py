@@ -153,6 +153,38 @@ def dist_setup():
     return world, rank, local
 
 
+# FP32 CUDA-core peak of a B200 (nominal): 148 SMs x 128 FP32 lanes x 2 flops
+# per FMA x 1.965 GHz.
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def factorization_flops(ns: int, nv: int) -> float:
+    """Flops of one real + one complex stage factorization of the block-banded
+    LU (nv x nv blocks, 3 off-diagonal blocks a side): per block row with nr
+    off-diagonal blocks, (1 + nr)^2 block products of 2 nv^3 flops (the
+    pivot inverse, nr L and nr W products, nr^2 Schur updates), and 4x that
+    for the complex system.  Half-width blocks hold the same band and cost
+    the same within the band's edges."""
+    rows = sum((1 + min(3, ns - 1 - i)) ** 2 for i in range(ns))
+    return 5.0 * 2.0 * nv ** 3 * rows
+
+
+def factorization_roofline(sinfo, radau_ms: float) -> dict:
+    """The stage factorizations' FP32 CUDA-core rate: their algorithmic flops
+    (factorization_flops x factorizations, per solve) over the Radau kernel's
+    time, and over the SM time the factorizations themselves took (the
+    per-solve phase timers, summed over solves and spread over the 148 SMs)."""
+    flops = float(sum(int(r[13]) * factorization_flops(int(r[7]), int(r[8])) for r in sinfo if r[7] > 0))
+    fac_share = float(sinfo[:, 18].sum()) / max(1.0, float(sinfo[:, 21].sum()))
+    ach = flops / (radau_ms / 1000.0) / 1e12
+    in_fac = ach / max(fac_share, 1e-9)
+    return {"bound": "fp32_fma", "kernel": "k_radau (stage factorizations)", "achieved": ach,
+            "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": ach / FP32_PEAK_TFLOPS,
+            "peak_kind": "nominal (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)",
+            "algorithmic_flops": flops, "factorization_share_of_kernel": fac_share,
+            "achieved_during_factorization": in_fac, "frac_during_factorization": in_fac / FP32_PEAK_TFLOPS}
+
+
 def cpu_baseline_run(P, I, rtol, n_threads, idx=None):
     """The oracle port on the contracts idx (all when None): one solve per
     thread, solves spread over n_threads host threads, the same discretization
@@ -218,6 +250,8 @@ def main():
                     help="skip the surrogate inference rate in the batch line")
     ap.add_argument("--no-cf-check", dest="cf_check", action="store_false",
                     help="skip the characteristic-function check and rate in the batch line")
+    ap.add_argument("--no-barrier", dest="barrier", action="store_false",
+                    help="skip the knock-in workload's compact summary in the batch line")
     ap.add_argument("--plain-sample", type=int, default=8,
                     help="contracts timed on the plain one-solve-per-launch FP64 path")
     ap.add_argument("--workload", default="batch", choices=["batch", "barrier", "surrogate", "calibration"],
@@ -294,6 +328,7 @@ def main():
     # per-kernel times and the roofline of the dominant kernel (k_radau)
     ktimes = plan.kernel_times(sptr)
     stats = plan.stats()
+    sinfo = plan.solve_info()
     # ---- device-resident timed region ------------------------------------------
     if world > 1:
         dist.barrier()
@@ -338,6 +373,7 @@ def main():
     radau_ms = ktimes[3]
     achieved = stats["factor_bytes"] / (radau_ms / 1000.0) / 1e9
     traffic = load_traffic()
+    fp32 = factorization_roofline(sinfo, radau_ms)
     # ---- CPU baseline (oracle port), rank 0, bounded sample -------------------------
     # The sample is two contracts of each of the nine grid classes; its oracle
     # prices also give this run's error against the FP64 oracle.
@@ -423,6 +459,12 @@ def main():
                "note": "discretization error of the FPE prices (the tight-tolerance FP64 run of the same "
                        "batch; floor 1e-3 S0) against the FP64 characteristic-function price; cf_rate: "
                        "k_heston_cf on 2^18 device-resident prices"}
+    # ---- the knock-in workload (config 2), compact: 1 warm-up run, 1 timed run -------
+    barrier = None
+    if rank == 0 and world == 1 and args.barrier:
+        barrier = barrier_measure(fpe, torch, stream, 1, 1, args.precision, args.rtol, args.seed)
+        barrier["note"] = ("1024 knock-in contracts (2048 solves, grids 48-96 x 24-48) in one launch sequence; "
+                           "one warm-up and one timed run; full measurement: bench.py --workload barrier")
     # ---- plain path: one contract per launch sequence, FP64 factors ---------------
     plain = None
     if rank == 0 and world == 1 and args.plain_sample > 0:
@@ -468,6 +510,8 @@ def main():
                          "peak_kind": peak_kind,
                          "traffic": traffic.get("bytes_per_launch") if traffic else None,
                          "algorithmic_bytes": int(stats["factor_bytes"])},
+            "roofline_fp32_factorization": fp32,
+            "barrier_knock_in": barrier,
             "cpu_baseline": cpu,
             "plain_fp64_one_per_launch": plain,
             "surrogate_inference": sur,
@@ -644,6 +688,56 @@ def make_barrier_batch(n: int, seed: int):
     return P, I
 
 
+def barrier_measure(fpe, torch, stream, steps: int, warmup: int, precision: int, rtol: float, seed: int,
+                    sub_n: int = 32, tight: bool = False) -> dict:
+    """The knock-in workload on one GPU: 1024 contracts (2048 solves, grids up
+    to 96 x 48, both solves of a pair at the default 0.01 x rtol) in one launch
+    sequence, timed with CUDA events on `stream` after `warmup` runs.  Error:
+    the mixed-precision prices of a sub_n-contract subsample against the FP64
+    path at the same tolerances (the same algorithm as the CPU oracle), and
+    with tight=True also against FP64 at rtol 1e-10."""
+    nc = 1024
+    P, I = make_barrier_batch(nc, seed)
+    opts = fpe.BatchOptions(disc=1, precision=precision, rtol=rtol, atol=rtol * 1e-2,
+                            complex_solve=2, radau_constants=2)
+    arr, keep = fpe.contracts_from_arrays(P, I)
+    plan = fpe.Plan(arr, opts, _keep=keep)
+    sptr = stream.cuda_stream
+    for _ in range(warmup):
+        plan.run(sptr)
+    torch.cuda.synchronize()
+    ktimes = plan.kernel_times(sptr)
+    stats = plan.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_launch = 0
+    e0.record(stream)
+    for _ in range(steps):
+        n_launch += plan.run(sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    p_out, _, _, _, st = plan.results()
+    plan.close()
+    sub = np.arange(0, nc, nc // sub_n)
+    floor = 1e-6 * 100.0
+    ref, st_ref = fpe.price_batch(P[sub], I[sub], fpe.BatchOptions(
+        disc=1, precision=0, rtol=rtol, atol=rtol * 1e-2, complex_solve=2, radau_constants=2))
+    rel = np.abs(p_out[sub] - ref) / np.maximum(np.abs(ref), floor)
+    out = {"value": nc / (ms / 1000.0), "unit": "prices/s", "ms_per_step": ms, "steps": steps, "warmup": warmup,
+           "contracts": nc, "solves": int(stats["solves"]), "rtol": rtol, "knock_in_tol_scale": 0.01,
+           "max_rel_err_vs_fp64_same_tol": float(rel.max()), "subsample": int(len(sub)), "err_floor": floor,
+           "status_ok": bool((st == 0).all() and (st_ref == 0).all()), "gpu_launches": n_launch,
+           "kernel_ms": {"setup": ktimes[0], "galerkin": ktimes[1], "ic": ktimes[2], "radau": ktimes[3],
+                         "payoff": ktimes[4]},
+           "solver": {k: int(v) for k, v in stats.items()}}
+    if tight:
+        tref, _ = fpe.price_batch(P[sub], I[sub], fpe.BatchOptions(
+            disc=1, precision=0, rtol=1e-10, atol=1e-12, complex_solve=2, radau_constants=2,
+            knock_in_tol_scale=1.0))
+        out["max_rel_err_vs_fp64_rtol1e-10"] = float((np.abs(p_out[sub] - tref) / np.maximum(np.abs(tref), floor)).max())
+    return out
+
+
 def run_barrier_workload(args):
     import torch
 
@@ -653,52 +747,25 @@ def run_barrier_workload(args):
     build.build_library()
     if not fpe.is_available():
         raise RuntimeError("CUDA engine unavailable")
-    nc = 1024
-    P, I = make_barrier_batch(nc, args.seed)
-    opts = fpe.BatchOptions(disc=1, precision=args.precision, rtol=args.rtol, atol=args.rtol * 1e-2,
-                            complex_solve=2, radau_constants=2)
-    arr, keep = fpe.contracts_from_arrays(P, I)
-    plan = fpe.Plan(arr, opts, _keep=keep)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    sptr = stream.cuda_stream
-    for _ in range(max(args.warmup, 3)):
-        plan.run(sptr)
-    torch.cuda.synchronize()
-    p_out, _, _, _, st = plan.results()
-    ktimes = plan.kernel_times(sptr)
-    stats = plan.stats()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    n_launch = 0
     with ClockSampler(0) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            n_launch += plan.run(sptr)
-        e1.record(stream)
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    # accuracy on a subsample against FP64 at a tight tolerance
-    sub = np.arange(0, nc, nc // 64)
-    ref, st_ref = fpe.price_batch(P[sub], I[sub], fpe.BatchOptions(
-        disc=1, precision=0, rtol=1e-10, atol=1e-12, complex_solve=2, radau_constants=2))
-    floor = 1e-6 * 100.0
-    rel = np.abs(p_out[sub] - ref) / np.maximum(np.abs(ref), floor)
+        m = barrier_measure(fpe, torch, stream, args.steps, max(args.warmup, 3), args.precision, args.rtol,
+                            args.seed, sub_n=64, tight=True)
     line = {"metric": "FPE knock-in prices/sec on 1 B200 (in-out parity, two solves each)",
-            "value": nc / (ms / 1000.0), "unit": "prices/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "dtype": "f32-factors/f64" if args.precision == 1 else "f64", "data": "synthetic",
+            "value": m["value"], "unit": "prices/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": m["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "dtype": "f32-factors/f64" if args.precision == 1 else "f64", "data": "synthetic",
             "workload": "barrier",
-            "config": {"workload": f"{nc} knock-in contracts ({stats['solves']} solves), grids 48-96 x 24-48, "
-                                   "one launch sequence", "rtol": args.rtol,
-                       "max_rel_err_vs_fp64_subsample": float(rel.max()), "subsample": int(len(sub)),
-                       "err_floor": floor, "status_ok": bool((st == 0).all() and (st_ref == 0).all())},
-            "gpu_launches": n_launch,
-            "kernel_ms": {"setup": ktimes[0], "galerkin": ktimes[1], "ic": ktimes[2], "radau": ktimes[3],
-                          "payoff": ktimes[4]},
-            "solver": {k: int(v) for k, v in stats.items()}, "clocks": clk.summary()}
+            "config": {"workload": f"1024 knock-in contracts ({m['solves']} solves), grids 48-96 x 24-48, "
+                                   "one launch sequence", **{k: m[k] for k in ("rtol", "knock_in_tol_scale",
+                                   "max_rel_err_vs_fp64_same_tol", "max_rel_err_vs_fp64_rtol1e-10", "subsample",
+                                   "err_floor", "status_ok")}},
+            "gpu_launches": m["gpu_launches"], "kernel_ms": m["kernel_ms"], "solver": m["solver"],
+            "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
-    plan.close()
     return 0
+
 
 def C_SIZE_CONTRACT():
     import ctypes

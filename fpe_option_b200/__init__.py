@@ -542,9 +542,9 @@ class Plan:
         return int(self._L.fpe_plan_retried(self._h))
 
     def solve_info(self) -> np.ndarray:
-        """Per-solve counters of the last run, (n_solves, 32) int32 in the plan's
+        """Per-solve counters of the last run, (n_solves, 40) int32 in the plan's
         solve order (see fpe_plan_solve_info in include/fpe_engine.h)."""
-        out = np.zeros((self.n_solves, 32), np.int32)
+        out = np.zeros((self.n_solves, 40), np.int32)
         if self._L.fpe_plan_solve_info(self._h, out.ctypes.data_as(_lib.ip)) < 0:
             raise RuntimeError("fpe_plan_solve_info failed")
         return out

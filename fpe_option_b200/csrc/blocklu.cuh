@@ -148,6 +148,26 @@ __device__ void blu_assemble(const OpFactors& O, const BlockLU<ET>& L, double a_
     const int k = i + kk - bw;
     if (k < 0 || k >= nb) continue;
     ET* B = L.F + size_t(blk) * bs;
+    if (b == nv) {  // nv x nv blocks: one s-coupling per block, rows and columns are v-dofs
+      const int sb = i * 7 + kk - bw + 3;
+      const double as = O.As[sb], ss = O.Ss[sb], ts = O.Ts[sb], st = O.St[sb];
+      for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+        const int j = int((float(e) + 0.5f) * rb), l = e - j * nv;
+        const int dl = l - j + 3;
+        double m = 0.0, kv = 0.0;
+        if (dl >= 0 && dl < 7) {
+          const int vb = j * 7 + dl;
+          m = as * O.Av[vb];
+          kv = ss * O.B1[vb] + ts * O.B2[vb] + as * O.B3[vb] + st * O.B4[vb];
+        }
+        if constexpr (!IsCx<ET>::v) {
+          st_elem(B[e], a_re * m + h * kv);
+        } else {
+          st_elem(B[e], cmk(a_re * m + h * kv, a_im * m));
+        }
+      }
+      continue;
+    }
     for (int e = threadIdx.x; e < nn; e += blockDim.x) {
       const int jj = int((float(e) + 0.5f) * rb), ll = e - jj * b;
       // global row r = i b + jj = si nv + vj and column c = k b + ll = sk nv + vl
@@ -248,6 +268,7 @@ struct FacScratch {
   ET* pinv;      // inverse pivot value of each column
   int* prow_of;  // pivot row of each column
   int* q_of;     // column whose pivot row is r
+  int* claim;    // work counter of the overlapped Schur updates
   int nv, nvp, ldt, w1;
   bool shared;   // scratch in shared memory (async staging possible)
   __device__ void init(ET* base, int b, int bw) {
@@ -267,6 +288,7 @@ struct FacScratch {
     pinv = pbuf + 2 * p;
     prow_of = reinterpret_cast<int*>(pinv + p);
     q_of = prow_of + p;
+    claim = q_of + p;
   }
 };
 
@@ -275,8 +297,11 @@ struct FacScratch {
 // real arithmetic per operand pair either way).
 template <typename ET>
 struct TileM { static constexpr int v = 4; };
+#ifndef FPE_CTILE_M
+#define FPE_CTILE_M 2
+#endif
 template <typename T>
-struct TileM<Cx<T>> { static constexpr int v = 2; };
+struct TileM<Cx<T>> { static constexpr int v = FPE_CTILE_M; };
 constexpr int kTileN = 4;
 
 // Vector loads/stores of K consecutive elements from 16-byte aligned shared memory.
@@ -329,6 +354,13 @@ __device__ __forceinline__ void vst16(double* p, const double (&v)[4]) {
 }
 __device__ __forceinline__ void vst16(Cx<float>* p, const Cx<float> (&v)[2]) {
   *reinterpret_cast<float4*>(p) = make_float4(v[0].re, v[0].im, v[1].re, v[1].im);
+}
+__device__ __forceinline__ void vst16(Cx<float>* p, const Cx<float> (&v)[4]) {
+  reinterpret_cast<float4*>(p)[0] = make_float4(v[0].re, v[0].im, v[1].re, v[1].im);
+  reinterpret_cast<float4*>(p)[1] = make_float4(v[2].re, v[2].im, v[3].re, v[3].im);
+}
+__device__ __forceinline__ void vst16(Cx<double>* p, const Cx<double> (&v)[4]) {
+  for (int q = 0; q < 4; ++q) reinterpret_cast<double2*>(p)[q] = make_double2(v[q].re, v[q].im);
 }
 __device__ __forceinline__ void vst16(Cx<double>* p, const Cx<double> (&v)[2]) {
   reinterpret_cast<double2*>(p)[0] = make_double2(v[0].re, v[0].im);
@@ -689,13 +721,20 @@ __device__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
 // (the next pivot block E_{i+1, i+1}) goes with TO_AUG into the Gauss-Jordan
 // array instead of the factor storage: the next block row inverts it from
 // there, and the factor storage of that block receives its inverse.
+template <typename ET>
+__device__ __forceinline__ int fac_tiles(const FacScratch<ET>& S) {
+  return (S.nvp / TileM<ET>::v) * (S.nvp / kTileN);
+}
+
+// Tile q of the Schur jobs job_lo, job_lo + 1, ... (q = job offset x tiles per
+// job + tile).
 template <typename ET, bool TO_AUG>
-__device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, int job_lo, int job_hi, int lt,
-                           int nt) {
+__device__ __forceinline__ void fac_update_tile(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, int job_lo,
+                                                int q) {
   constexpr int TM = TileM<ET>::v;
   const int nv = S.nv, p = S.nvp, t = S.ldt;
-  const int tr = p / TM, tc = p / kTileN, ntile = tr * tc;
-  for (int q = lt; q < (job_hi - job_lo) * ntile; q += nt) {
+  const int tc = p / kTileN, ntile = fac_tiles(S);
+  {
     const int jq = q / ntile, tt = q - jq * ntile, job = job_lo + jq;
     const int j0 = (tt / tc) * TM, l0 = (tt - (tt / tc) * tc) * kTileN;
     const int rr = job / nr, cc = job - rr * nr;
@@ -719,6 +758,35 @@ __device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int n
 #pragma unroll
         for (int n = 0; n < kTileN; ++n)
           if (j0 + m < nv && l0 + n < nv) E[(j0 + m) * nv + l0 + n] = acc[m][n];
+    }
+  }
+}
+
+template <typename ET, bool TO_AUG>
+__device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, int job_lo, int job_hi, int lt,
+                           int nt) {
+  for (int q = lt; q < (job_hi - job_lo) * fac_tiles(S); q += nt) fac_update_tile<ET, TO_AUG>(L, S, i, nr, job_lo, q);
+}
+
+// Schur updates 1 .. nr^2 - 1 of both systems (real tiles first), claimed 32
+// tiles at a time per warp from a shared counter, so that the warps which
+// finish their pivot inverse early take their share of the products.
+template <typename FT>
+__device__ void fac_update_claim(const BlockLU<FT>& LR, FacScratch<FT>& SR, const BlockLU<Cx<FT>>* LC,
+                                 FacScratch<Cx<FT>>& SC, int i, int nr, int* ctr) {
+  const int lane = threadIdx.x & 31;
+  const int nr_tiles = (nr * nr - 1) * fac_tiles(SR);
+  const int total = nr_tiles + (LC ? (nr * nr - 1) * fac_tiles(SC) : 0);
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(ctr, 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= total) break;
+    const int q = base + lane;
+    if (q < nr_tiles) {
+      fac_update_tile<FT, false>(LR, SR, i, nr, 1, q);
+    } else if (q < total) {
+      fac_update_tile<Cx<FT>, false>(*LC, SC, i, nr, 1, q - nr_tiles);
     }
   }
 }
@@ -781,6 +849,7 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
           SC.prow_of[r] = r;
         }
       }
+      if (threadIdx.x == 0) *SR.claim = 0;
       __syncthreads();
       const long long t3 = clock64();
       tcyc[1] += t3 - t2;
@@ -789,11 +858,8 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
           ok &= FPE_GJ<FT>(SR);
         } else if (warp == 1) {
           if (LC) ok &= FPE_GJ<Cx<FT>>(SC);
-        } else {
-          const int lt = threadIdx.x - 64, nt = blockDim.x - 64;
-          fac_update<FT, false>(LR, SR, i, nr, 1, nr * nr, lt, nt);
-          if (LC) fac_update<Cx<FT>, false>(*LC, SC, i, nr, 1, nr * nr, lt, nt);
         }
+        fac_update_claim<FT>(LR, SR, LC, SC, i, nr, SR.claim);
         // this warp's own time in the overlapped phase, before the barrier
         tcyc[2] += clock64() - t3;
       } else {
@@ -990,6 +1056,8 @@ struct SolveStage {
   int slot_r, slot_c;        // bytes per staged real / complex block slot
   long long wait_limit;      // SM cycles a stage waits for its copies
   long long* wait_cycles;    // accumulates this thread's cycles spent in those waits
+  long long* work_cycles;    // ... in a stage's work after the wait
+  long long* bar_cycles;     // ... at the stage barriers
 };
 
 __host__ __device__ __forceinline__ int stage_slot_bytes(int b, int esz) {
@@ -1023,12 +1091,12 @@ __device__ __forceinline__ const ET* stage_block(const BlockLU<ET>& L, int s, in
 // Issues the bulk copies of stage s.  gfence orders the factor's earlier
 // generic-proxy writes (the factorization) before the async-proxy reads; the
 // factor does not change during a sweep, so only a sweep's first issue needs it.
-template <typename FT>
+template <typename FT, int BW>
 __device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s, int b, bool gfence) {
   unsigned long long* bar = P.bar + b;
   unsigned char* dst = P.buf[b];
   const int nv = S.R ? S.R->b : S.Cf->b;  // block size
-  const int ng = (S.R ? S.R->bw : S.Cf->bw) + 1;
+  constexpr int ng = BW + 1;
   const uint32_t br = uint32_t(fpe_block_stride(nv)) * sizeof(FT);
   const uint32_t bc = 2 * br;
   uint32_t bytes = 0;
@@ -1137,14 +1205,16 @@ __device__ __forceinline__ void col_dot_c(const Cx<T>* col, const double* xr, co
 // is carried across calls (a sweep leaves every barrier with an even number
 // of completed phases or not: each thread tracks them); every thread of the
 // CTA calls this.
-template <typename FT>
-__device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uint32_t& phase) {
+// BW: the factor's off-diagonal blocks per side (3 or 7), a template
+// parameter so that the per-stage block loops unroll.
+template <typename FT, int BW>
+__device__ bool blu_solve_staged_bw(const SolveSet<FT>& S, const SolveStage& P, uint32_t& phase) {
   if (*P.err) return false;
   const int ns = S.R ? S.R->nb : S.Cf->nb;  // block rows
   const int nv = S.R ? S.R->b : S.Cf->b;    // block size
-  const int bw = S.R ? S.R->bw : S.Cf->bw;
-  const int ng = bw + 1;                    // slots per stage
-  const int rmask = ring_segments(bw) - 1;
+  constexpr int bw = BW;
+  constexpr int ng = bw + 1;                // slots per stage
+  constexpr int rmask = (bw < 4 ? 4 : 8) - 1;
   const int nstage = 2 * ns + 1;
   const int tid = threadIdx.x;
   // roles
@@ -1170,7 +1240,7 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
   uint32_t pend = 0;  // buffers with a stage in flight (the issuer's view)
   if (tid == issuer) {
     for (int q = 0; q < nbuf && q < nstage; ++q) {
-      stage_issue<FT>(S, P, q, q, q == 0);
+      stage_issue<FT, BW>(S, P, q, q, q == 0);
       pend |= 1u << q;
     }
   }
@@ -1275,13 +1345,16 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
         }
       }
     }
+    const long long tb0 = clock64();
+    *P.work_cycles += tb0 - tw0;
     __syncthreads();
+    *P.bar_cycles += clock64() - tb0;
     if (*P.err) {
       ok = false;
       break;
     }
     if (tid == issuer && s + nbuf < nstage) {
-      stage_issue<FT>(S, P, s + nbuf, b, false);
+      stage_issue<FT, BW>(S, P, s + nbuf, b, false);
       pend |= 1u << b;
     }
   }
@@ -1293,6 +1366,12 @@ __device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uin
   }
   __syncthreads();
   return ok;
+}
+
+template <typename FT>
+__device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uint32_t& phase) {
+  const int bw = S.R ? S.R->bw : S.Cf->bw;
+  return bw == 7 ? blu_solve_staged_bw<FT, 7>(S, P, phase) : blu_solve_staged_bw<FT, 3>(S, P, phase);
 }
 
 }  // namespace fpe

@@ -46,7 +46,11 @@ enum FpeInfo {
   FPE_INFO_T_GJ_REAL, FPE_INFO_T_GJ_CPLX, FPE_INFO_T_SCHUR,
   FPE_INFO_T_FASM,    // inside T_FACTOR: stage-matrix assembly (kilocycles)
   FPE_INFO_T_FSTAGE,  // inside T_FACTOR: staging of each block row and the pivot-inverse extraction
-  FPE_INFO_COUNT = 32
+  // inside T_SOLVE (kilocycles): a stage's work after its copies landed, up
+  // to the stage barrier, for thread 0 (a real row) and for the first thread
+  // of the complex rows; and thread 0's wait at the stage barrier
+  FPE_INFO_T_SREAL, FPE_INFO_T_SCPLX, FPE_INFO_T_SBAR,
+  FPE_INFO_COUNT = 40
 };
 
 struct FpeSolveDesc {

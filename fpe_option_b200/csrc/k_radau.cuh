@@ -258,8 +258,10 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
   SP.bar = S.pipe_bar;
   SP.err = &S.pipe_err;
   SP.wait_limit = d.stage_wait > 0 ? (long long)d.stage_wait : kBulkWaitLimit;
-  long long t_swait = 0;
+  long long t_swait = 0, t_swork = 0, t_sbar = 0;
   SP.wait_cycles = &t_swait;
+  SP.work_cycles = &t_swork;
+  SP.bar_cycles = &t_sbar;
   uint32_t pipe_phase = 0;
   const KronTerm Kt[4] = {{O.Ss, O.B1, 1.0}, {O.Ts, O.B2, 1.0}, {O.As, O.B3, 1.0}, {O.St, O.B4, 1.0}};
   const KronTerm Mt[1] = {{O.As, O.Av, 1.0}};
@@ -831,8 +833,13 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
     info[FPE_INFO_T_GJ_REAL] = int(t_fsub[2] >> 10);
     info[FPE_INFO_T_FASM] = int(t_fasm >> 10);
     info[FPE_INFO_T_FSTAGE] = int(t_fsub[3] >> 10);
+    info[FPE_INFO_T_SREAL] = int((t_swork - t_swait) >> 10);
+    info[FPE_INFO_T_SBAR] = int(t_sbar >> 10);
   }
-  if (threadIdx.x == 32) info[FPE_INFO_T_GJ_CPLX] = int(t_fsub[2] >> 10);
+  if (threadIdx.x == 32) {
+    info[FPE_INFO_T_GJ_CPLX] = int(t_fsub[2] >> 10);
+    info[FPE_INFO_T_SCPLX] = int((t_swork - t_swait) >> 10);
+  }
   if (threadIdx.x == 64) info[FPE_INFO_T_SCHUR] = int(t_fsub[2] >> 10);
 }
 

@@ -260,7 +260,7 @@ extern int32_t fpe_tune_get(int32_t disc, int32_t n_s, int32_t n_v, int32_t prec
 extern void fpe_tune_clear(void);
 
 /** Number of words per solve in fpe_plan_solve_info. */
-#define FPE_SOLVE_INFO_WORDS 32
+#define FPE_SOLVE_INFO_WORDS 40
 /** Per-solve counters of the plan's last run, FPE_SOLVE_INFO_WORDS words per
  *  solve in the plan's solve order (longest estimated solve first): 0 status,
  *  7-8 dofs (s, v), 9 accepted, 10 rejected, 11 Newton, 12 GMRES, 13 LU
@@ -271,7 +271,8 @@ extern void fpe_tune_clear(void);
  *  overlapped factorization phase's own work of the real pivot inverse, the
  *  complex pivot inverse and the other Schur updates, 28 the stage
  *  matrices' assembly, 29 the block rows' staging and pivot-inverse
- *  extraction.  out holds
+ *  extraction, 30-32 the sweeps' stage work of a real row and of a complex
+ *  row and a real row's wait at the stage barriers.  out holds
  *  n_solves * FPE_SOLVE_INFO_WORDS words.  Returns n_solves, < 0 on error. */
 extern int32_t fpe_plan_solve_info(FpePlan* plan, int32_t* out);
 extern void fpe_plan_destroy(FpePlan* plan);
