@@ -25,6 +25,16 @@
 #include "dev_common.cuh"
 #include "bulk_pipe.cuh"
 
+// The dynamic shared memory of the launch.  Pointers formed from it keep
+// their shared address space through inlining, so their loads are LDS; a
+// pointer carried through a struct member is generic and its loads take the
+// slower generic path (long scoreboard).
+extern __shared__ __align__(16) unsigned char fpe_dsmem[];
+
+__device__ __forceinline__ uint32_t dsmem_offset(const void* p) {
+  return uint32_t(reinterpret_cast<const unsigned char*>(p) - fpe_dsmem);
+}
+
 // The pivot-block inverse used by the factorization (fac_gj: registers for FP32
 // blocks where it can; fac_gj_warp: shared-memory rows).
 #ifndef FPE_GJ
@@ -132,45 +142,92 @@ struct BlockLU {
   __device__ __forceinline__ ET* blk(int i, int kk) const { return F + (size_t(i) * (2 * bw + 1) + kk) * bs; }
 };
 
-// E = (a_re + i a_im) M + h K into the block storage (a_im ignored for real ET).
-template <typename ET>
-__device__ void blu_assemble(const OpFactors& O, const BlockLU<ET>& L, double a_re, double a_im,
-                             double h) {
-  // Block by block: the blocks of a block row whose column lies outside the
-  // matrix (k < 0 or k >= nb) are never read, by the factorization or by the
-  // sweeps, and are not written; the padding after a block's b^2 entries is
-  // not read either.  Rows and columns come from the exact float reciprocal
-  // (arguments below 2^16), not from integer divisions.
-  const int nb = L.nb, b = L.b, nv = O.nv, bs = L.bs, bw = L.bw, w = 2 * bw + 1, nn = b * b;
+// Four consecutive elements to a 16-byte-aligned address with 16-byte stores.
+__device__ __forceinline__ void store4(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void store4(double* p, const double (&v)[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void store4(Cx<float>* p, const Cx<float> (&v)[4]) {
+  reinterpret_cast<float4*>(p)[0] = make_float4(v[0].re, v[0].im, v[1].re, v[1].im);
+  reinterpret_cast<float4*>(p)[1] = make_float4(v[2].re, v[2].im, v[3].re, v[3].im);
+}
+__device__ __forceinline__ void store4(Cx<double>* p, const Cx<double> (&v)[4]) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) reinterpret_cast<double2*>(p)[k] = make_double2(v[k].re, v[k].im);
+}
+
+// E_r = a_r M + h K into LR and, when cplx, E_c = (c_re + i c_im) M + h K into
+// LC, in one pass over the blocks (both need the same entries of M and K).
+// Compiled as a function of its own: the operator factors (shared memory) and
+// the block descriptions arrive by value and are read into registers once, so
+// that no read in the loop goes to the kernel's stack frame (whose slots the
+// compiler must reload after every store through a global pointer).  The
+// blocks of a block row whose column lies outside the matrix (k < 0 or
+// k >= nb) are never read, by the factorization or by the sweeps, and are not
+// written; neither is the padding after a block's b^2 entries.  Rows and
+// columns inside a block come from the exact float reciprocal (arguments
+// below 2^16), not from integer divisions.
+template <typename FT>
+__device__ __noinline__ void blu_assemble_pair(OpFactors O, BlockLU<FT> LR, BlockLU<Cx<FT>> LC, bool cplx,
+                                               double a_r, double c_re, double c_im, double h) {
+  // the factors as shared-memory pointers (they live in the launch's dynamic
+  // shared memory), so that their loads are LDS
+  auto sh = [](const double* p) { return reinterpret_cast<const double*>(fpe_dsmem + dsmem_offset(p)); };
+  const double *As = sh(O.As), *Ss = sh(O.Ss), *Ts = sh(O.Ts), *St = sh(O.St);
+  const double *Av = sh(O.Av), *B1 = sh(O.B1), *B2 = sh(O.B2), *B3 = sh(O.B3), *B4 = sh(O.B4);
+  FT* const FR = LR.F;
+  Cx<FT>* const FC = LC.F;
+  const int nb = LR.nb, b = LR.b, nv = O.nv, bs = LR.bs, bw = LR.bw, w = 2 * bw + 1, nn = b * b;
   const float rb = 1.0f / float(b), rnv = 1.0f / float(nv);
-  for (int blk = 0; blk < nb * w; ++blk) {
-    const int i = blk / w, kk = blk - w * i;
-    const int k = i + kk - bw;
-    if (k < 0 || k >= nb) continue;
-    ET* B = L.F + size_t(blk) * bs;
-    if (b == nv) {  // nv x nv blocks: one s-coupling per block, rows and columns are v-dofs
+  if (b == nv && (nv & 3) == 0) {
+    // nv x nv blocks, nv a multiple of 4: one s-coupling per block, rows and
+    // columns are v-dofs, nonzero only on the 7 diagonals |j - l| <= 3.  A
+    // thread fills 4 consecutive entries of a row (16-byte-aligned vector
+    // stores) and computes only those on the band.  Work items q run over
+    // (block, chunk) pairs.
+    const int cpr = nv >> 2, nch = nn >> 2;
+    const float rcpr = 1.0f / float(cpr);
+    const int total = nb * w * nch;
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+      const int blk = q / nch, ch = q - blk * nch;
+      const int i = blk / w, kk = blk - w * i;
+      const int k = i + kk - bw;
+      if (k < 0 || k >= nb) continue;
+      const int j = int((float(ch) + 0.5f) * rcpr), l0 = (ch - j * cpr) << 2;
       const int sb = i * 7 + kk - bw + 3;
-      const double as = O.As[sb], ss = O.Ss[sb], ts = O.Ts[sb], st = O.St[sb];
-      for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-        const int j = int((float(e) + 0.5f) * rb), l = e - j * nv;
-        const int dl = l - j + 3;
+      FT vr[4];
+      Cx<FT> vc[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int dl = l0 + u - j + 3;
         double m = 0.0, kv = 0.0;
         if (dl >= 0 && dl < 7) {
           const int vb = j * 7 + dl;
-          m = as * O.Av[vb];
-          kv = ss * O.B1[vb] + ts * O.B2[vb] + as * O.B3[vb] + st * O.B4[vb];
+          const double as = As[sb];
+          m = as * Av[vb];
+          kv = Ss[sb] * B1[vb] + Ts[sb] * B2[vb] + as * B3[vb] + St[sb] * B4[vb];
         }
-        if constexpr (!IsCx<ET>::v) {
-          st_elem(B[e], a_re * m + h * kv);
-        } else {
-          st_elem(B[e], cmk(a_re * m + h * kv, a_im * m));
-        }
+        vr[u] = FT(a_r * m + h * kv);
+        vc[u] = cmk(FT(c_re * m + h * kv), FT(c_im * m));
       }
-      continue;
+      const size_t off = size_t(blk) * bs + size_t(j) * nv + l0;
+      store4(FR + off, vr);
+      if (cplx) store4(FC + off, vc);
     }
-    for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+  } else {
+    // general blocks (b = nv / m): entry (jj, ll) of block (i, kk) is the
+    // coupling of global row r = i b + jj = si nv + vj and column
+    // c = k b + ll = sk nv + vl
+    const int total = nb * w * nn;
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+      const int blk = q / nn, e = q - blk * nn;
+      const int i = blk / w, kk = blk - w * i;
+      const int k = i + kk - bw;
+      if (k < 0 || k >= nb) continue;
       const int jj = int((float(e) + 0.5f) * rb), ll = e - jj * b;
-      // global row r = i b + jj = si nv + vj and column c = k b + ll = sk nv + vl
       const int r = i * b + jj, c = k * b + ll;
       const int si = int((float(r) + 0.5f) * rnv), vj = r - si * nv;
       const int sk = int((float(c) + 0.5f) * rnv), vl = c - sk * nv;
@@ -178,15 +235,13 @@ __device__ void blu_assemble(const OpFactors& O, const BlockLU<ET>& L, double a_
       double m = 0.0, kv = 0.0;
       if (ds >= 0 && ds < 7 && dl >= 0 && dl < 7) {
         const int sb = si * 7 + ds, vb = vj * 7 + dl;
-        const double as = O.As[sb];
-        m = as * O.Av[vb];
-        kv = O.Ss[sb] * O.B1[vb] + O.Ts[sb] * O.B2[vb] + as * O.B3[vb] + O.St[sb] * O.B4[vb];
+        const double as = As[sb];
+        m = as * Av[vb];
+        kv = Ss[sb] * B1[vb] + Ts[sb] * B2[vb] + as * B3[vb] + St[sb] * B4[vb];
       }
-      if constexpr (!IsCx<ET>::v) {
-        st_elem(B[e], a_re * m + h * kv);
-      } else {
-        st_elem(B[e], cmk(a_re * m + h * kv, a_im * m));
-      }
+      const size_t off = size_t(blk) * bs + e;
+      FR[off] = FT(a_r * m + h * kv);
+      if (cplx) FC[off] = cmk(FT(c_re * m + h * kv), FT(c_im * m));
     }
   }
   __syncthreads();
@@ -426,7 +481,7 @@ __device__ __forceinline__ void stage_elem(ET* dst, const ET* src) {
 // array, and the pivot bookkeeping reset), with REST the nr U blocks of row i
 // and E blocks of column i.
 template <typename ET, bool ASYNC>
-__device__ void fac_stage_impl(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, bool pivot, bool rest) {
+__device__ __forceinline__ void fac_stage_impl(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, bool pivot, bool rest) {
   const int nv = S.nv, nn = nv * nv, w1 = S.w1, p = S.nvp, t = S.ldt;
   const float rnv = 1.0f / float(nv);
   if (pivot) {
@@ -459,7 +514,7 @@ __device__ void fac_stage_impl(const BlockLU<ET>& L, FacScratch<ET>& S, int i, i
 }
 
 template <typename ET>
-__device__ void fac_stage(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, bool pivot = true,
+__device__ __forceinline__ void fac_stage(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, bool pivot = true,
                           bool rest = true) {
   if (S.shared) {
     fac_stage_impl<ET, true>(L, S, i, nr, pivot, rest);
@@ -492,7 +547,7 @@ __device__ __forceinline__ unsigned pivot_key(float m, int r) {
 // its columns in pivot order (column q_l holds inverse column l).  Returns
 // false for a zero or non-finite pivot.
 template <typename ET>
-__device__ bool fac_gj_warp(FacScratch<ET>& S) {
+__device__ __forceinline__ bool fac_gj_warp(FacScratch<ET>& S) {
   const int lane = threadIdx.x & 31, nv = S.nv, w1 = S.w1;
   const int r0 = lane, r1 = lane + 32;
   const bool own0 = r0 < nv, own1 = r1 < nv;
@@ -556,9 +611,17 @@ __device__ bool fac_gj_warp(FacScratch<ET>& S) {
 // steps the columns are back in order.  The pivot choice, the arithmetic of
 // each element and the bookkeeping are those of fac_gj_warp.
 template <typename ET, int NV>
-__device__ __noinline__ bool fac_gj_warp_reg(FacScratch<ET>& S) {
+__device__ __noinline__ bool fac_gj_warp_reg(uint32_t aug_off, uint32_t pbuf_off, uint32_t pinv_off,
+                                              uint32_t prow_off, uint32_t qof_off) {
   static_assert(NV <= 32 && NV % 4 == 0, "register rows of up to 32 columns, 16-byte chunks");
-  const int lane = threadIdx.x & 31, w1 = S.w1;
+  // the scratch arrays, rebuilt from shared offsets so that their accesses are LDS / STS
+  struct {
+    ET *aug, *pbuf, *pinv;
+    int *prow_of, *q_of;
+  } S{reinterpret_cast<ET*>(fpe_dsmem + aug_off), reinterpret_cast<ET*>(fpe_dsmem + pbuf_off),
+      reinterpret_cast<ET*>(fpe_dsmem + pinv_off), reinterpret_cast<int*>(fpe_dsmem + prow_off),
+      reinterpret_cast<int*>(fpe_dsmem + qof_off)};
+  const int lane = threadIdx.x & 31, w1 = NV + 1;
   const bool own = lane < NV;
   ET row[NV];
 #pragma unroll
@@ -621,15 +684,19 @@ struct IsF32Elem<Cx<float>> { static constexpr bool v = true; };
 // The pivot-block inverse: rows in registers for FP32 blocks of 8 to 32
 // columns (multiples of 4), rows in shared memory otherwise.
 template <typename ET>
-__device__ bool fac_gj(FacScratch<ET>& S) {
+__device__ __forceinline__ bool fac_gj(FacScratch<ET>& S) {
   if constexpr (IsF32Elem<ET>::v) {
-    switch (S.nv) {
-      case 8: return fac_gj_warp_reg<ET, 8>(S);
-      case 12: return fac_gj_warp_reg<ET, 12>(S);
-      case 16: return fac_gj_warp_reg<ET, 16>(S);
-      case 24: return fac_gj_warp_reg<ET, 24>(S);
-      case 32: return fac_gj_warp_reg<ET, 32>(S);
-      default: break;
+    if (S.shared) {
+      const uint32_t a = dsmem_offset(S.aug), pb = dsmem_offset(S.pbuf), pi = dsmem_offset(S.pinv),
+                     pr = dsmem_offset(S.prow_of), qo = dsmem_offset(S.q_of);
+      switch (S.nv) {
+        case 8: return fac_gj_warp_reg<ET, 8>(a, pb, pi, pr, qo);
+        case 12: return fac_gj_warp_reg<ET, 12>(a, pb, pi, pr, qo);
+        case 16: return fac_gj_warp_reg<ET, 16>(a, pb, pi, pr, qo);
+        case 24: return fac_gj_warp_reg<ET, 24>(a, pb, pi, pr, qo);
+        case 32: return fac_gj_warp_reg<ET, 32>(a, pb, pi, pr, qo);
+        default: break;
+      }
     }
   }
   return fac_gj_warp<ET>(S);
@@ -638,7 +705,7 @@ __device__ bool fac_gj(FacScratch<ET>& S) {
 // P^-1 (row k = row p_k of the array scaled by 1 / a_{p_k k}, columns
 // un-permuted) into Pi, PiT and the factor storage.
 template <typename ET>
-__device__ void fac_extract(const BlockLU<ET>& L, FacScratch<ET>& S, int i) {
+__device__ __forceinline__ void fac_extract(const BlockLU<ET>& L, FacScratch<ET>& S, int i) {
   const int nv = S.nv, w1 = S.w1, p = S.nvp, t = S.ldt;
   const float rnv = 1.0f / float(nv);
   ET* g = L.blk(i, L.bw);
@@ -664,7 +731,7 @@ __device__ void fac_extract(const BlockLU<ET>& L, FacScratch<ET>& S, int i) {
 // one output column are contiguous in the transposed storage: one vector
 // store each, and a warp's stores cover contiguous memory.
 template <typename ET>
-__device__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
+__device__ __forceinline__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
   constexpr int TM = TileM<ET>::v;
   const int nv = S.nv, p = S.nvp, t = S.ldt;
   const int tr = p / TM, tc = p / kTileN, ntile = tr * tc;
@@ -763,7 +830,7 @@ __device__ __forceinline__ void fac_update_tile(const BlockLU<ET>& L, FacScratch
 }
 
 template <typename ET, bool TO_AUG>
-__device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, int job_lo, int job_hi, int lt,
+__device__ __forceinline__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, int job_lo, int job_hi, int lt,
                            int nt) {
   for (int q = lt; q < (job_hi - job_lo) * fac_tiles(S); q += nt) fac_update_tile<ET, TO_AUG>(L, S, i, nr, job_lo, q);
 }
@@ -772,7 +839,7 @@ __device__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int n
 // tiles at a time per warp from a shared counter, so that the warps which
 // finish their pivot inverse early take their share of the products.
 template <typename FT>
-__device__ void fac_update_claim(const BlockLU<FT>& LR, FacScratch<FT>& SR, const BlockLU<Cx<FT>>* LC,
+__device__ __forceinline__ void fac_update_claim(const BlockLU<FT>& LR, FacScratch<FT>& SR, const BlockLU<Cx<FT>>* LC,
                                  FacScratch<Cx<FT>>& SC, int i, int nr, int* ctr) {
   const int lane = threadIdx.x & 31;
   const int nr_tiles = (nr * nr - 1) * fac_tiles(SR);
@@ -795,9 +862,10 @@ __device__ void fac_update_claim(const BlockLU<FT>& LR, FacScratch<FT>& SR, cons
 // lockstep so both share every barrier).  scr_r / scr_c: scratch of
 // fpe_fac_scratch_elems(b, bw) elements each.
 template <typename FT>
-__device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC, FT* scr_r,
+__device__ __forceinline__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC, FT* scr_r,
                                 Cx<FT>* scr_c, long long (&tcyc)[4]) {
   const int ns = LR.nb, bw = LR.bw;  // block rows, off-diagonal blocks
+  long long tc0 = 0, tc1 = 0, tc2 = 0, tc3 = 0;  // phase timers in registers, added to tcyc at the end
   FacScratch<FT> SR;
   SR.init(scr_r, LR.b, bw);
   FacScratch<Cx<FT>> SC;
@@ -819,7 +887,7 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
     if (warp == 0) ok &= FPE_GJ<FT>(SR);
     else if (warp == 1 && LC) ok &= FPE_GJ<Cx<FT>>(SC);
     __syncthreads();
-    tcyc[0] += clock64() - t0;
+    tc0 += clock64() - t0;
   }
   for (int i = 0; i < ns; ++i) {
     const int nr = min(i + bw, ns - 1) - i;
@@ -832,7 +900,7 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
     fac_extract<FT>(LR, SR, i);
     if (LC) fac_extract<Cx<FT>>(*LC, SC, i);
     __syncthreads();
-    tcyc[3] += clock64() - t1;
+    tc3 += clock64() - t1;
     if (nr > 0) {
       const long long t2 = clock64();
       fac_lw<FT>(LR, SR, i, nr);
@@ -852,7 +920,7 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
       if (threadIdx.x == 0) *SR.claim = 0;
       __syncthreads();
       const long long t3 = clock64();
-      tcyc[1] += t3 - t2;
+      tc1 += t3 - t2;
       if (split) {
         if (warp == 0) {
           ok &= FPE_GJ<FT>(SR);
@@ -861,7 +929,7 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
         }
         fac_update_claim<FT>(LR, SR, LC, SC, i, nr, SR.claim);
         // this warp's own time in the overlapped phase, before the barrier
-        tcyc[2] += clock64() - t3;
+        tc2 += clock64() - t3;
       } else {
         fac_update<FT, false>(LR, SR, i, nr, 1, nr * nr, threadIdx.x, blockDim.x);
         if (LC) fac_update<Cx<FT>, false>(*LC, SC, i, nr, 1, nr * nr, threadIdx.x, blockDim.x);
@@ -870,18 +938,54 @@ __device__ bool blu_factor_pair(const BlockLU<FT>& LR, const BlockLU<Cx<FT>>* LC
         else if (warp == 1 && LC) ok &= FPE_GJ<Cx<FT>>(SC);
       }
       __syncthreads();
-      tcyc[0] += clock64() - t3;
+      tc0 += clock64() - t3;
     }
   }
+  tcyc[0] += tc0;
+  tcyc[1] += tc1;
+  tcyc[2] += tc2;
+  tcyc[3] += tc3;
   return __syncthreads_and(ok ? 1 : 0) != 0;  // the same verdict in every thread
 }
 
+// The factorization with its scratch in shared memory, compiled as a
+// function of its own: it gets a register allocation of its own (the kernel
+// around it is large), its block descriptions arrive by value, and its
+// scratch as shared-window offsets, so that no read in its loops goes to the
+// kernel's stack frame and every scratch access is a shared-memory
+// instruction.  tcyc accumulates the phase timers of blu_factor_pair.
+template <typename FT>
+__device__ __noinline__ bool blu_factor_pair_smem(BlockLU<FT> LR, BlockLU<Cx<FT>> LC, bool cplx, uint32_t scr_r,
+                                                  uint32_t scr_c, long long* tcyc) {
+  long long tc[4] = {0, 0, 0, 0};
+  const bool ok = blu_factor_pair<FT>(LR, cplx ? &LC : nullptr, reinterpret_cast<FT*>(fpe_dsmem + scr_r),
+                                      reinterpret_cast<Cx<FT>*>(fpe_dsmem + scr_c), tc);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) tcyc[k] += tc[k];
+  return ok;
+}
+
+// The same with the scratch in global memory (blocks too wide for shared
+// memory), also out of line.
+template <typename FT>
+__device__ __noinline__ bool blu_factor_pair_gmem(BlockLU<FT> LR, BlockLU<Cx<FT>> LC, bool cplx, FT* scr_r,
+                                                  Cx<FT>* scr_c, long long* tcyc) {
+  long long tc[4] = {0, 0, 0, 0};
+  const bool ok = blu_factor_pair<FT>(LR, cplx ? &LC : nullptr, scr_r, scr_c, tc);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) tcyc[k] += tc[k];
+  return ok;
+}
+
 // Right-hand sides of one fused solve: up to two real vectors on the real
-// factor and one complex vector (re, im arrays) on the complex factor.
+// factor and one complex vector (re, im arrays) on the complex factor.  The
+// factors' descriptions are held by value (both share their block structure;
+// R's describes it); the staged solve reads the members it needs into scalars
+// once per sweep.
 template <typename FT>
 struct SolveSet {
-  const BlockLU<FT>* R;
-  const BlockLU<Cx<FT>>* Cf;
+  BlockLU<FT> R;
+  BlockLU<Cx<FT>> Cf;
   double* xr[2];   // in: b, out: x
   double* zr[2];   // scratch N
   int nr;
@@ -930,10 +1034,11 @@ __device__ __forceinline__ Cx<double> grp_dot<Cx<double>, Cx<double>>(const Cx<d
 // groups of G lanes own one row of one system; every lane executes the same
 // shuffle reductions (real systems carry a zero imaginary part).
 template <typename FT>
-__device__ void blu_solve(const SolveSet<FT>& S) {
-  const int ns = S.R ? S.R->nb : S.Cf->nb;  // block rows
-  const int nv = S.R ? S.R->b : S.Cf->b;    // block size
-  const int bw = S.R ? S.R->bw : S.Cf->bw;
+__device__ __forceinline__ void blu_solve(const SolveSet<FT>& Sin) {
+  const SolveSet<FT> S = Sin;  // in registers for the sweep
+  const int ns = S.R.nb;   // block rows
+  const int nv = S.R.b;    // block size
+  const int bw = S.R.bw;
   const int rows = (S.nr + S.nc) * nv;
   int G = 32;
   while (G > 1 && rows * G > int(blockDim.x)) G >>= 1;
@@ -955,14 +1060,14 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
   for (int i = 0; i <= ns; ++i) {
     double ar = 0.0, ai = 0.0, zr = 0.0, zi = 0.0;
     if (is_r) {
-      const BlockLU<FT>& L = *S.R;
+      const BlockLU<FT>& L = S.R;
       const double* x = S.xr[sys];
       if (i < ns)
         for (int k = 1; k <= bw && i - k >= 0; ++k)
           ar += grp_dot<FT, double>(L.blk(i, bw - k) + j, x + (i - k) * nv, nullptr, nv, gl, G);
       if (i > 0) zr = grp_dot<FT, double>(L.blk(i - 1, bw) + j, x + (i - 1) * nv, nullptr, nv, gl, G);
     } else if (is_c) {
-      const BlockLU<Cx<FT>>& L = *S.Cf;
+      const BlockLU<Cx<FT>>& L = S.Cf;
       if (i < ns)
         for (int k = 1; k <= bw && i - k >= 0; ++k) {
           const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i, bw - k) + j, S.xc_re + (i - k) * nv,
@@ -999,12 +1104,12 @@ __device__ void blu_solve(const SolveSet<FT>& S) {
   for (int i = ns - 1; i >= 0; --i) {
     double ar = 0.0, ai = 0.0, d0 = 0.0, d1 = 0.0;
     if (is_r) {
-      const BlockLU<FT>& L = *S.R;
+      const BlockLU<FT>& L = S.R;
       const double* x = S.xr[sys];
       for (int k = 1; k <= bw && i + k < ns; ++k)
         ar += grp_dot<FT, double>(L.blk(i, bw + k) + j, x + (i + k) * nv, nullptr, nv, gl, G);
     } else if (is_c) {
-      const BlockLU<Cx<FT>>& L = *S.Cf;
+      const BlockLU<Cx<FT>>& L = S.Cf;
       for (int k = 1; k <= bw && i + k < ns; ++k) {
         const Cx<double> d = grp_dot<Cx<FT>, Cx<double>>(L.blk(i, bw + k) + j, S.xc_re + (i + k) * nv,
                                                          S.xc_im + (i + k) * nv, nv, gl, G);
@@ -1058,6 +1163,10 @@ struct SolveStage {
   long long* wait_cycles;    // accumulates this thread's cycles spent in those waits
   long long* work_cycles;    // ... in a stage's work after the wait
   long long* bar_cycles;     // ... at the stage barriers
+  bool rhs_bulk;             // forward stages bring their right-hand-side segments along
+                             // (block size even: 16-byte aligned segments)
+  void* zbuf;                // shared z = P^-1 y of the forward sweep (null: global scratch)
+  int zcap;                  // bytes of zbuf
 };
 
 __host__ __device__ __forceinline__ int stage_slot_bytes(int b, int esz) {
@@ -1065,84 +1174,163 @@ __host__ __device__ __forceinline__ int stage_slot_bytes(int b, int esz) {
 }
 // Segments of the sweep's ring: bw + 1 rounded up to a power of two.
 __host__ __device__ __forceinline__ int ring_segments(int bw) { return bw < 4 ? 4 : 8; }
-// Bytes of one stage buffer (bw + 1 slots) for block size b, element size esz
-// of the real factor, with or without the complex factor.
-__host__ __device__ __forceinline__ int stage_bytes(int b, int esz, bool cplx, int bw) {
+// Bytes of one stage buffer for block size b, element size esz of the real
+// factor, with or without the complex factor: bw + 1 factor-block slots, then
+// up to four right-hand-side segments of b doubles (offset stage_rhs_offset).
+__host__ __device__ __forceinline__ int stage_rhs_offset(int b, int esz, bool cplx, int bw) {
   return (bw + 1) * (stage_slot_bytes(b, esz) + (cplx ? stage_slot_bytes(b, 2 * esz) : 0));
+}
+__host__ __device__ __forceinline__ int stage_bytes(int b, int esz, bool cplx, int bw) {
+  return stage_rhs_offset(b, esz, cplx, bw) + ((4 * b * 8 + 15) & ~15);
 }
 // Bytes of nbuf stage buffers plus the ring (up to 4 arrays of 8-byte entries).
 __host__ __device__ __forceinline__ int stage_total_bytes(int b, int esz, bool cplx, int bw, int nbuf) {
   return nbuf * stage_bytes(b, esz, cplx, bw) + ring_segments(bw) * b * 4 * 8;
 }
 
-// Block (row, kk) of stage s and slot g; nullptr when the row has no such block.
-template <typename ET>
-__device__ __forceinline__ const ET* stage_block(const BlockLU<ET>& L, int s, int g) {
-  const int nb = L.nb, bw = L.bw;
-  if (s <= nb) {
-    const int i = s;
-    if (g < bw) return (i < nb && i - bw + g >= 0) ? L.blk(i, g) : nullptr;
-    return i >= 1 ? L.blk(i - 1, bw) : nullptr;
-  }
-  const int i = 2 * nb - s;
-  return (g < bw && i + 1 + g < nb) ? L.blk(i, bw + 1 + g) : nullptr;
-}
-
-// Issues the bulk copies of stage s.  gfence orders the factor's earlier
-// generic-proxy writes (the factorization) before the async-proxy reads; the
-// factor does not change during a sweep, so only a sweep's first issue needs it.
+// The copies of a sweep's stages as the issuing thread sees them: factor
+// bases, shared-window addresses of the stage buffers and their barriers, and
+// the right-hand sides, all scalars.  No member is an array, so nothing is
+// indexed at run time and the whole description stays in registers (a
+// run-time index into a struct array places it in local memory, whose loads
+// miss the small L1 left beside a large shared-memory carve-out and would put
+// hundreds of cycles on every stage).
 template <typename FT, int BW>
-__device__ void stage_issue(const SolveSet<FT>& S, const SolveStage& P, int s, int b, bool gfence) {
-  unsigned long long* bar = P.bar + b;
-  unsigned char* dst = P.buf[b];
-  const int nv = S.R ? S.R->b : S.Cf->b;  // block size
-  constexpr int ng = BW + 1;
-  const uint32_t br = uint32_t(fpe_block_stride(nv)) * sizeof(FT);
-  const uint32_t bc = 2 * br;
-  uint32_t bytes = 0;
-  for (int g = 0; g < ng; ++g) {
-    if (S.nr > 0 && stage_block(*S.R, s, g)) bytes += br;
-    if (S.nc > 0 && stage_block(*S.Cf, s, g)) bytes += bc;
+struct StageCopies {
+  const unsigned char* fr;  // real factor (bytes); null: no real system
+  const unsigned char* fc;  // complex factor (bytes); null: no complex system
+  uint32_t br;              // bytes per real block (a complex block is 2 br)
+  int nb;                   // block rows
+  uint32_t dst0, dstep;     // shared address of stage buffer 0, bytes between buffers
+  uint32_t slot_r, slot_c;  // bytes per staged real / complex block slot
+  uint32_t rhs_at;          // offset of the right-hand-side segments in a buffer
+  uint32_t bar0;            // shared address of barrier 0 (8 bytes per barrier)
+  uint32_t seg;             // bytes of one right-hand-side segment (b doubles)
+  const double *x0, *x1, *xre, *xim;  // right-hand sides (null: none)
+  bool rhs;                 // forward stages bring their right-hand-side segments
+
+  // Block kk of factor row i as a byte offset from the factor base.
+  __device__ __forceinline__ size_t boff(int i, int kk, uint32_t bb) const {
+    return (size_t(i) * (2 * BW + 1) + kk) * bb;
   }
-  fence_proxy_async_smem();
-  if (gfence) fence_proxy_async_global();
-  if (bytes == 0) {
-    mbar_arrive(bar);
-    return;
-  }
-  mbar_arrive_expect_tx(bar, bytes);
-  for (int g = 0; g < ng; ++g) {
-    if (S.nr > 0) {
-      const FT* src = stage_block(*S.R, s, g);
-      if (src) bulk_g2s(dst + g * P.slot_r, src, br, bar);
+  // Slot g of stage s: whether the row has the block, and its (row, column
+  // slot).  Forward row i = s <= nb: L_{i,i-BW+g} for g < BW, P^-1_{i-1} for
+  // g = BW; backward row i = 2 nb - s: W_{i,i+1+g} for g < BW.
+  __device__ __forceinline__ bool slot(int s, int g, int& i, int& kk) const {
+    if (s <= nb) {
+      if (g < BW) {
+        i = s;
+        kk = g;
+        return s < nb && s - BW + g >= 0;
+      }
+      i = s - 1;
+      kk = BW;
+      return s >= 1;
     }
-    if (S.nc > 0) {
-      const Cx<FT>* src = stage_block(*S.Cf, s, g);
-      if (src) bulk_g2s(dst + ng * P.slot_r + g * P.slot_c, src, bc, bar);
+    i = 2 * nb - s;
+    kk = BW + 1 + g;
+    return g < BW && i + 1 + g < nb;
+  }
+  // Issues the copies of stage s into buffer b.  gfence orders the factor's
+  // earlier generic-proxy writes (the factorization) before the async-proxy
+  // reads; the factor does not change during a sweep, so only a sweep's first
+  // issue needs it.
+  __device__ __forceinline__ void issue(int s, int b, bool gfence) const {
+    constexpr int ng = BW + 1;
+    const uint32_t bar = bar0 + 8u * uint32_t(b);
+    const uint32_t dst = dst0 + uint32_t(b) * dstep;
+    const bool rrow = rhs && s < nb;  // forward rows 0 .. nb-1 read b_s
+    int nblk = 0;
+#pragma unroll
+    for (int g = 0; g < ng; ++g) {
+      int i, kk;
+      nblk += slot(s, g, i, kk) ? 1 : 0;
+    }
+    const int nrhs = rrow ? (x0 ? 1 : 0) + (x1 ? 1 : 0) + (xre ? 2 : 0) : 0;
+    const uint32_t bytes = uint32_t(nblk) * ((fr ? br : 0u) + (fc ? 2 * br : 0u)) + uint32_t(nrhs) * seg;
+    fence_proxy_async_smem();
+    if (gfence) fence_proxy_async_global();
+    if (bytes == 0) {
+      mbar_arrive_u32(bar);
+      return;
+    }
+    mbar_arrive_expect_tx_u32(bar, bytes);
+#pragma unroll
+    for (int g = 0; g < ng; ++g) {
+      int i, kk;
+      if (!slot(s, g, i, kk)) continue;
+      if (fr) bulk_g2s_u32(dst + uint32_t(g) * slot_r, fr + boff(i, kk, br), br, bar);
+      if (fc) bulk_g2s_u32(dst + uint32_t(ng) * slot_r + uint32_t(g) * slot_c, fc + boff(i, kk, 2 * br), 2 * br, bar);
+    }
+    if (rrow) {
+      uint32_t r = dst + rhs_at;
+      const size_t o = size_t(s) * (seg >> 3);
+      if (x0) { bulk_g2s_u32(r, x0 + o, seg, bar); r += seg; }
+      if (x1) { bulk_g2s_u32(r, x1 + o, seg, bar); r += seg; }
+      if (xre) {
+        bulk_g2s_u32(r, xre + o, seg, bar);
+        bulk_g2s_u32(r + seg, xim + o, seg, bar);
+      }
     }
   }
-}
+};
 
 // a += sum_m col[m nv] x[m] with independent accumulators (col: shared,
 // transposed block).  With FP32 factors the sweep accumulates in FP32: the
 // factor's own rounding is of the same order, and the FP64 Newton residual
 // corrects whatever the preconditioner apply leaves.
+// With nv a multiple of 4 (x then 16-byte aligned in the ring) x is read in
+// 16-byte vectors, one broadcast load per four products; the sums are the
+// same either way.
 __device__ __forceinline__ void col_dot(const float* col, const float* x, int nv, float& a) {
   float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
   int m = 0;
-  for (; m + 3 < nv; m += 4) {
-    a0 = fmaf(col[m * nv], x[m], a0);
-    a1 = fmaf(col[(m + 1) * nv], x[m + 1], a1);
-    a2 = fmaf(col[(m + 2) * nv], x[m + 2], a2);
-    a3 = fmaf(col[(m + 3) * nv], x[m + 3], a3);
+  if ((nv & 3) == 0) {
+    for (; m < nv; m += 4) {
+      const float4 xv = *reinterpret_cast<const float4*>(x + m);
+      a0 = fmaf(col[m * nv], xv.x, a0);
+      a1 = fmaf(col[(m + 1) * nv], xv.y, a1);
+      a2 = fmaf(col[(m + 2) * nv], xv.z, a2);
+      a3 = fmaf(col[(m + 3) * nv], xv.w, a3);
+    }
+  } else {
+    for (; m + 3 < nv; m += 4) {
+      a0 = fmaf(col[m * nv], x[m], a0);
+      a1 = fmaf(col[(m + 1) * nv], x[m + 1], a1);
+      a2 = fmaf(col[(m + 2) * nv], x[m + 2], a2);
+      a3 = fmaf(col[(m + 3) * nv], x[m + 3], a3);
+    }
+    for (; m < nv; ++m) a0 = fmaf(col[m * nv], x[m], a0);
   }
-  for (; m < nv; ++m) a0 = fmaf(col[m * nv], x[m], a0);
   a += (a0 + a1) + (a2 + a3);
 }
 __device__ __forceinline__ void col_dot_c(const Cx<float>* col, const float* xr, const float* xi, int nv, float& ar,
                                           float& ai) {
   float r0 = 0.f, r1 = 0.f, i0 = 0.f, i1 = 0.f;
   int m = 0;
+  if ((nv & 3) == 0) {
+    for (; m < nv; m += 4) {
+      const float4 xr4 = *reinterpret_cast<const float4*>(xr + m);
+      const float4 xi4 = *reinterpret_cast<const float4*>(xi + m);
+      const Cx<float> b0 = col[m * nv], b1 = col[(m + 1) * nv], b2 = col[(m + 2) * nv], b3 = col[(m + 3) * nv];
+      r0 = fmaf(b0.re, xr4.x, r0);
+      r0 = fmaf(-b0.im, xi4.x, r0);
+      i0 = fmaf(b0.re, xi4.x, i0);
+      i0 = fmaf(b0.im, xr4.x, i0);
+      r1 = fmaf(b1.re, xr4.y, r1);
+      r1 = fmaf(-b1.im, xi4.y, r1);
+      i1 = fmaf(b1.re, xi4.y, i1);
+      i1 = fmaf(b1.im, xr4.y, i1);
+      r0 = fmaf(b2.re, xr4.z, r0);
+      r0 = fmaf(-b2.im, xi4.z, r0);
+      i0 = fmaf(b2.re, xi4.z, i0);
+      i0 = fmaf(b2.im, xr4.z, i0);
+      r1 = fmaf(b3.re, xr4.w, r1);
+      r1 = fmaf(-b3.im, xi4.w, r1);
+      i1 = fmaf(b3.re, xi4.w, i1);
+      i1 = fmaf(b3.im, xr4.w, i1);
+    }
+  }
   for (; m + 1 < nv; m += 2) {
     const Cx<float> b0 = col[m * nv], b1 = col[(m + 1) * nv];
     r0 = fmaf(b0.re, xr[m], r0);
@@ -1200,6 +1388,29 @@ __device__ __forceinline__ void col_dot_c(const Cx<T>* col, const double* xr, co
   ai += i0;
 }
 
+// What slot g of block row i multiplies: forward rows take L_{i,i-bw+g}
+// (g < bw) times the solved segment i - bw + g into the L sum, and P^-1_{i-1}
+// (g = bw) times segment i - 1 into z; backward rows take W_{i,i+1+g} (g < bw)
+// times segment i + 1 + g.  valid: the row has that block.
+struct StageSlot {
+  int seg;
+  bool valid, to_z;
+};
+template <int BW>
+__device__ __forceinline__ StageSlot stage_slot(bool fwd, int i, int ns, int g) {
+  StageSlot q;
+  if (fwd) {
+    q.to_z = g >= BW;
+    q.seg = q.to_z ? i - 1 : i - BW + g;
+    q.valid = q.to_z ? i >= 1 : (i < ns && q.seg >= 0);
+  } else {
+    q.to_z = false;
+    q.seg = i + 1 + g;
+    q.valid = g < BW && q.seg < ns;
+  }
+  return q;
+}
+
 // Returns false when a bounded wait gave up (the solve result is then invalid
 // and *P.err is set).  `phase` holds the parity bits of the nbuf barriers and
 // is carried across calls (a sweep leaves every barrier with an even number
@@ -1208,83 +1419,162 @@ __device__ __forceinline__ void col_dot_c(const Cx<T>* col, const double* xr, co
 // BW: the factor's off-diagonal blocks per side (3 or 7), a template
 // parameter so that the per-stage block loops unroll.
 template <typename FT, int BW>
-__device__ bool blu_solve_staged_bw(const SolveSet<FT>& S, const SolveStage& P, uint32_t& phase) {
+__device__ __noinline__ bool blu_solve_staged_bw(const SolveSet<FT>& S, const SolveStage& P,
+                                                    uint32_t& phase) {
   if (*P.err) return false;
-  const int ns = S.R ? S.R->nb : S.Cf->nb;  // block rows
-  const int nv = S.R ? S.R->b : S.Cf->b;    // block size
+  // The set's and the stage's members as scalars, read once: the loop below
+  // indexes nothing of S or P at run time (see StageCopies).
+  const int ns = S.R.nb;  // block rows
+  const int nv = S.R.b;   // block size
+  const int nr = S.nr, nc = S.nc;
   constexpr int bw = BW;
   constexpr int ng = bw + 1;                // slots per stage
   constexpr int rmask = (bw < 4 ? 4 : 8) - 1;
   const int nstage = 2 * ns + 1;
   const int tid = threadIdx.x;
-  // roles
-  const int nreal = S.nr * nv;
-  const int cbase = (nreal + 31) & ~31;
+  // roles: Gr lanes own one row of a real system and Gc lanes one row of the
+  // complex system, each lane the slots g = its lane, + G, ... of the stage;
+  // real rows first, the complex ones from the next warp boundary, and at
+  // least one thread left over to issue the copies where the block allows
+  const int nreal = nr * nv;
+  const int nthr = int(blockDim.x);
   int Gc = 4;
-  while (Gc > 1 && cbase + Gc * nv > int(blockDim.x)) Gc >>= 1;
-  const bool is_r = tid < nreal;
-  const int rsys = is_r ? tid / nv : 0;
-  const int rj = is_r ? tid - rsys * nv : 0;
-  const bool is_c = S.nc > 0 && tid >= cbase && tid < cbase + Gc * nv;
+  while (Gc > 1 && ((nreal + 31) & ~31) + Gc * nv > nthr) Gc >>= 1;
+  const int ncthr = nc > 0 ? Gc * nv : 0;
+  int Gr = 4;
+  while (Gr > 1 && ((nreal * Gr + 31) & ~31) + ncthr > nthr - 1) Gr >>= 1;
+  const int cbase = (nreal * Gr + 31) & ~31;
+  const bool is_r = tid < nreal * Gr;
+  const int rrow = is_r ? tid / Gr : 0, rg = is_r ? tid - rrow * Gr : 0;
+  const int rsys = is_r ? rrow / nv : 0;
+  const int rj = is_r ? rrow - rsys * nv : 0;
+  const bool is_c = nc > 0 && tid >= cbase && tid < cbase + ncthr;
   const int cu = is_c ? tid - cbase : 0;
   const int cj = cu / Gc, cg = cu - cj * Gc;
+  double* const xr_me = rsys ? S.xr[1] : S.xr[0];  // this thread's real system's vectors
+  double* const zr_me = rsys ? S.zr[1] : S.zr[0];
+  double* const xc_re = S.xc_re;
+  double* const xc_im = S.xc_im;
+  double* const zc_re = S.zc_re;
+  double* const zc_im = S.zc_im;
   using RT = FT;  // accumulation / ring type: float with FP32 factors, double with FP64
-  const int rlen = (rmask + 1) * nv;  // ring length per right-hand-side array
-  RT* ringb = static_cast<RT*>(P.ring);
-  RT* ring_c_re = ringb + S.nr * rlen;
+  // ring segments of rs entries: FP32 segments are padded by four entries, so
+  // that the segments which the lanes of a warp read together start in
+  // different banks (the ring area is sized for FP64 entries, which this fits)
+  const int rs = nv + (sizeof(RT) == 4 ? 4 : 0);
+  const int rlen = (rmask + 1) * rs;  // ring length per right-hand-side array
+  // stage buffers, ring and z as shared-space pointers (see fpe_dsmem)
+  unsigned char* const sbuf0 = fpe_dsmem + dsmem_offset(P.buf[0]);
+  const uint32_t sstride = uint32_t(P.buf[1] - P.buf[0]);
+  const int slot_r = P.slot_r, slot_c = P.slot_c;
+  const bool rhs_bulk = P.rhs_bulk;
+  RT* ringb = reinterpret_cast<RT*>(fpe_dsmem + dsmem_offset(P.ring));
+  RT* ring_c_re = ringb + nr * rlen;
   RT* ring_c_im = ring_c_re + rlen;
+  // z of every block row in shared memory when it fits (real systems first,
+  // then the complex re and im parts), else in the global scratch vectors
+  const int N = ns * nv;
+  const bool zsh = P.zbuf && size_t(nr + 2 * nc) * N * sizeof(RT) <= size_t(P.zcap);
+  RT* zs = zsh ? reinterpret_cast<RT*>(fpe_dsmem + dsmem_offset(P.zbuf)) : nullptr;
+  RT* zs_re = zs + nr * N;
+  RT* zs_im = zs_re + N;
+  const int rhs_at = ng * (slot_r + (nc > 0 ? slot_c : 0));  // rhs segments in a stage buffer
+  int* const err = P.err;
 
   // the thread that issues the copies: an idle one when the roles leave one
-  const int issuer = (int(blockDim.x) - 1 >= max(nreal, cbase + (S.nc > 0 ? Gc * nv : 0))) ? int(blockDim.x) - 1 : 0;
+  const int issuer = (nthr - 1 >= max(nreal * Gr, cbase + ncthr)) ? nthr - 1 : 0;
   const int nbuf = P.nbuf;
+  StageCopies<FT, BW> cp;
+  if (tid == issuer) {
+    cp.fr = nr > 0 ? reinterpret_cast<const unsigned char*>(S.R.F) : nullptr;
+    cp.fc = nc > 0 ? reinterpret_cast<const unsigned char*>(S.Cf.F) : nullptr;
+    cp.br = uint32_t(S.R.bs) * uint32_t(sizeof(FT));
+    cp.nb = ns;
+    cp.dst0 = smem_u32(sbuf0);
+    cp.dstep = sstride;
+    cp.slot_r = uint32_t(slot_r);
+    cp.slot_c = uint32_t(slot_c);
+    cp.rhs_at = uint32_t(rhs_at);
+    cp.bar0 = smem_u32(P.bar);
+    cp.seg = uint32_t(nv) * 8u;
+    cp.x0 = nr > 0 ? S.xr[0] : nullptr;
+    cp.x1 = nr > 1 ? S.xr[1] : nullptr;
+    cp.xre = nc > 0 ? xc_re : nullptr;
+    cp.xim = nc > 0 ? xc_im : nullptr;
+    cp.rhs = rhs_bulk;
+  }
   uint32_t pend = 0;  // buffers with a stage in flight (the issuer's view)
   if (tid == issuer) {
     for (int q = 0; q < nbuf && q < nstage; ++q) {
-      stage_issue<FT, BW>(S, P, q, q, q == 0);
+      cp.issue(q, q, q == 0);
       pend |= 1u << q;
     }
   }
   bool ok = true;
+  // the barriers' parity bits and the timers stay in registers during the sweep
+  uint32_t ph = phase;
+  long long t_wait = 0, t_work = 0, t_bar = 0;
+  unsigned long long* const bars = P.bar;
+  const long long wlim = P.wait_limit;
   int b = 0;  // buffer of stage s: s mod nbuf
   for (int s = 0; s < nstage; ++s, b = (b + 1 == nbuf) ? 0 : b + 1) {
     const long long tw0 = clock64();
-    const bool landed = mbar_wait_bounded(P.bar + b, (phase >> b) & 1u, P.wait_limit);
-    *P.wait_cycles += clock64() - tw0;
+    const bool landed = mbar_wait_bounded(bars + b, (ph >> b) & 1u, wlim);
+    t_wait += clock64() - tw0;
     if (landed) {
-      phase ^= 1u << b;
+      ph ^= 1u << b;
       pend &= ~(1u << b);
     } else {
       ok = false;
-      *P.err = 1;
+      *err = 1;
     }
     ok = __all_sync(0xffffffffu, ok);  // uniform per warp before the group shuffles
-    const unsigned char* buf = P.buf[b];
+    const unsigned char* buf = sbuf0 + b * sstride;
     const bool fwd = s <= ns;
     const int i = fwd ? s : 2 * ns - s;
     if (ok) {
-      if (is_r) {
-        const RT* ring = ringb + rsys * rlen;
-        RT a = RT(0), z = RT(0);
+      RT a = RT(0), z = RT(0);  // real row: L products (forward) or W products, and P^-1 y
+      // the row's right-hand side (forward) or z (backward), loaded before the products
+      double xb = 0.0;
+      if (is_r && rg == 0) {
         if (fwd) {
-          // the right-hand side's row is loaded before the products
-          const double xb = i < ns ? S.xr[rsys][i * nv + rj] : 0.0;
-          for (int g = 0; g < bw; ++g)
-            if (i < ns && i - bw + g >= 0)
-              col_dot(reinterpret_cast<const FT*>(buf + g * P.slot_r) + rj, ring + ((i - bw + g) & rmask) * nv, nv,
-                      a);
-          if (i >= 1)
-            col_dot(reinterpret_cast<const FT*>(buf + bw * P.slot_r) + rj, ring + ((i - 1) & rmask) * nv, nv, z);
-          if (i < ns) ringb[rsys * rlen + (i & rmask) * nv + rj] = RT(xb - double(a));
-          if (i >= 1) S.zr[rsys][(i - 1) * nv + rj] = double(z);
+          if (i < ns) xb = rhs_bulk ? reinterpret_cast<const double*>(buf + rhs_at)[rsys * nv + rj] : xr_me[i * nv + rj];
         } else {
-          const double zb = S.zr[rsys][i * nv + rj];
-          for (int g = 0; g < bw; ++g)
-            if (i + 1 + g < ns)
-              col_dot(reinterpret_cast<const FT*>(buf + g * P.slot_r) + rj, ring + ((i + 1 + g) & rmask) * nv, nv,
-                      a);
-          const double x = zb - double(a);
-          ringb[rsys * rlen + (i & rmask) * nv + rj] = RT(x);
-          S.xr[rsys][i * nv + rj] = x;
+          xb = zsh ? double(zs[rsys * N + i * nv + rj]) : zr_me[i * nv + rj];
+        }
+      }
+      if (is_r) {
+        // one code path for every slot (the lanes of a warp hold different
+        // slots and stay converged): the slot's ring segment, and whether it
+        // feeds the L / W sum or P^-1 y
+        const RT* ring = ringb + rsys * rlen;
+        for (int g = rg; g < ng; g += Gr) {
+          const StageSlot q = stage_slot<bw>(fwd, i, ns, g);
+          if (q.valid) {
+            RT d = RT(0);
+            col_dot(reinterpret_cast<const FT*>(buf + g * slot_r) + rj, ring + (q.seg & rmask) * rs, nv, d);
+            if (q.to_z) z += d;
+            else a += d;
+          }
+        }
+      }
+      if (tid < cbase) {  // group reduction over the Gr lanes of a real row (real warps only)
+        for (int o = Gr >> 1; o > 0; o >>= 1) {
+          a += __shfl_down_sync(0xffffffffu, a, o, Gr);
+          z += __shfl_down_sync(0xffffffffu, z, o, Gr);
+        }
+      }
+      if (is_r && rg == 0) {
+        if (fwd) {
+          if (i < ns) ringb[rsys * rlen + (i & rmask) * rs + rj] = RT(xb - double(a));
+          if (i >= 1) {
+            if (zsh) zs[rsys * N + (i - 1) * nv + rj] = z;
+            else zr_me[(i - 1) * nv + rj] = double(z);
+          }
+        } else {
+          const double x = xb - double(a);
+          ringb[rsys * rlen + (i & rmask) * rs + rj] = RT(x);
+          xr_me[i * nv + rj] = x;
         }
       }
       RT ar = RT(0), ai = RT(0), zr = RT(0), zi = RT(0);
@@ -1292,69 +1582,83 @@ __device__ bool blu_solve_staged_bw(const SolveSet<FT>& S, const SolveStage& P, 
       double cre = 0.0, cim = 0.0;
       if (is_c && cg == 0) {
         if (!fwd) {
-          cre = S.zc_re[i * nv + cj];
-          cim = S.zc_im[i * nv + cj];
+          cre = zsh ? double(zs_re[i * nv + cj]) : zc_re[i * nv + cj];
+          cim = zsh ? double(zs_im[i * nv + cj]) : zc_im[i * nv + cj];
         } else if (i < ns) {
-          cre = S.xc_re[i * nv + cj];
-          cim = S.xc_im[i * nv + cj];
-        }
-      }
-      if (is_c) {
-        const unsigned char* cb = buf + ng * P.slot_r;
-        for (int g = cg; g < ng; g += Gc) {
-          const Cx<FT>* col = reinterpret_cast<const Cx<FT>*>(cb + g * P.slot_c) + cj;
-          if (fwd) {
-            if (g < bw) {
-              if (i < ns && i - bw + g >= 0) {
-                const int seg = ((i - bw + g) & rmask) * nv;
-                col_dot_c(col, ring_c_re + seg, ring_c_im + seg, nv, ar, ai);
-              }
-            } else if (i >= 1) {
-              const int seg = ((i - 1) & rmask) * nv;
-              col_dot_c(col, ring_c_re + seg, ring_c_im + seg, nv, zr, zi);
-            }
-          } else if (g < bw && i + 1 + g < ns) {
-            const int seg = ((i + 1 + g) & rmask) * nv;
-            col_dot_c(col, ring_c_re + seg, ring_c_im + seg, nv, ar, ai);
+          if (rhs_bulk) {
+            const double* rb = reinterpret_cast<const double*>(buf + rhs_at) + nr * nv;
+            cre = rb[cj];
+            cim = rb[nv + cj];
+          } else {
+            cre = xc_re[i * nv + cj];
+            cim = xc_im[i * nv + cj];
           }
         }
       }
-      // group reduction over the Gc lanes of a complex row (uniform in the warp)
-      for (int o = Gc >> 1; o > 0; o >>= 1) {
-        ar += __shfl_down_sync(0xffffffffu, ar, o, Gc);
-        ai += __shfl_down_sync(0xffffffffu, ai, o, Gc);
-        zr += __shfl_down_sync(0xffffffffu, zr, o, Gc);
-        zi += __shfl_down_sync(0xffffffffu, zi, o, Gc);
+      if (is_c) {
+        const unsigned char* cb = buf + ng * slot_r;
+        for (int g = cg; g < ng; g += Gc) {
+          const StageSlot q = stage_slot<bw>(fwd, i, ns, g);
+          if (q.valid) {
+            RT dr = RT(0), di = RT(0);
+            const int seg = (q.seg & rmask) * rs;
+            col_dot_c(reinterpret_cast<const Cx<FT>*>(cb + g * slot_c) + cj, ring_c_re + seg, ring_c_im + seg, nv, dr,
+                      di);
+            if (q.to_z) {
+              zr += dr;
+              zi += di;
+            } else {
+              ar += dr;
+              ai += di;
+            }
+          }
+        }
+      }
+      // group reduction over the Gc lanes of a complex row (complex warps only)
+      if (tid >= cbase) {
+        for (int o = Gc >> 1; o > 0; o >>= 1) {
+          ar += __shfl_down_sync(0xffffffffu, ar, o, Gc);
+          ai += __shfl_down_sync(0xffffffffu, ai, o, Gc);
+          zr += __shfl_down_sync(0xffffffffu, zr, o, Gc);
+          zi += __shfl_down_sync(0xffffffffu, zi, o, Gc);
+        }
       }
       if (is_c && cg == 0) {
         if (fwd) {
           if (i < ns) {
-            ring_c_re[(i & rmask) * nv + cj] = RT(cre - double(ar));
-            ring_c_im[(i & rmask) * nv + cj] = RT(cim - double(ai));
+            ring_c_re[(i & rmask) * rs + cj] = RT(cre - double(ar));
+            ring_c_im[(i & rmask) * rs + cj] = RT(cim - double(ai));
           }
           if (i >= 1) {
-            S.zc_re[(i - 1) * nv + cj] = double(zr);
-            S.zc_im[(i - 1) * nv + cj] = double(zi);
+            if (zsh) {
+              zs_re[(i - 1) * nv + cj] = zr;
+              zs_im[(i - 1) * nv + cj] = zi;
+            } else {
+              zc_re[(i - 1) * nv + cj] = double(zr);
+              zc_im[(i - 1) * nv + cj] = double(zi);
+            }
           }
         } else {
           const double xr = cre - double(ar), xi = cim - double(ai);
-          ring_c_re[(i & rmask) * nv + cj] = RT(xr);
-          ring_c_im[(i & rmask) * nv + cj] = RT(xi);
-          S.xc_re[i * nv + cj] = xr;
-          S.xc_im[i * nv + cj] = xi;
+          ring_c_re[(i & rmask) * rs + cj] = RT(xr);
+          ring_c_im[(i & rmask) * rs + cj] = RT(xi);
+          xc_re[i * nv + cj] = xr;
+          xc_im[i * nv + cj] = xi;
         }
       }
     }
     const long long tb0 = clock64();
-    *P.work_cycles += tb0 - tw0;
-    __syncthreads();
-    *P.bar_cycles += clock64() - tb0;
-    if (*P.err) {
+    t_work += tb0 - tw0;
+    // the stage barrier also tells every thread whether a wait gave up (the
+    // failing threads set *P.err, which the caller reads after the sweep)
+    const bool failed = __syncthreads_or(ok ? 0 : 1) != 0;
+    t_bar += clock64() - tb0;
+    if (failed) {
       ok = false;
       break;
     }
     if (tid == issuer && s + nbuf < nstage) {
-      stage_issue<FT, BW>(S, P, s + nbuf, b, false);
+      cp.issue(s + nbuf, b, false);
       pend |= 1u << b;
     }
   }
@@ -1362,15 +1666,19 @@ __device__ bool blu_solve_staged_bw(const SolveSet<FT>& S, const SolveStage& P, 
     // let copies still in flight land before the buffers are reused: the full
     // (about one second) limit, whatever the stage waits were given
     for (int q = 0; q < nbuf; ++q)
-      if ((pend >> q) & 1u) mbar_wait_bounded(P.bar + q, (phase >> q) & 1u, kBulkWaitLimit);
+      if ((pend >> q) & 1u) mbar_wait_bounded(bars + q, (ph >> q) & 1u, kBulkWaitLimit);
   }
+  phase = ph;
+  *P.wait_cycles += t_wait;
+  *P.work_cycles += t_work;
+  *P.bar_cycles += t_bar;
   __syncthreads();
   return ok;
 }
 
 template <typename FT>
-__device__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uint32_t& phase) {
-  const int bw = S.R ? S.R->bw : S.Cf->bw;
+__device__ __forceinline__ bool blu_solve_staged(const SolveSet<FT>& S, const SolveStage& P, uint32_t& phase) {
+  const int bw = S.R.bw;
   return bw == 7 ? blu_solve_staged_bw<FT, 7>(S, P, phase) : blu_solve_staged_bw<FT, 3>(S, P, phase);
 }
 

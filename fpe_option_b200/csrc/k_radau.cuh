@@ -116,7 +116,12 @@ static __device__ void kron_apply(const RadauCtx& C, const KronTerm* terms, int 
 }
 
 struct RadauSmem {
-  unsigned long long pipe_bar[kMaxStageBufs];  // stage-buffer barriers of the staged block solve
+  // The stage-buffer barriers of the staged block solve have a 128-byte line to
+  // themselves: the bulk copies' transaction counts update them from the async
+  // proxy, and an ordinary access to a word of the same line waits for those
+  // updates (thousands of cycles while a stage's copies are in flight).
+  alignas(128) unsigned long long pipe_bar[kMaxStageBufs];
+  unsigned long long pipe_bar_pad[16 - kMaxStageBufs];
   int pipe_err, pipe_pad;
   double red[32 * 8];
   double H[(FPE_GMRES_M + 1) * FPE_GMRES_M];
@@ -196,7 +201,7 @@ static __device__ void apply_E2(const RadauCtx& C, const KronTerm* Edt, const Kr
 
 template <typename FT>
 __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<FT> A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   RadauSmem& S = *reinterpret_cast<RadauSmem*>(smem_raw);
   const FpeSolveDesc d = A.descs[blockIdx.x];
   const FpeDLayout DL = fpe_dlayout(d);
@@ -240,14 +245,18 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
   // Staged sweeps when the stage buffers fit in the (shared) factorization
   // scratch, which is idle while the sweeps run.
   const long long fac_bytes = fac_shared ? (long long)fac_need : 0;
-  // As many stage buffers (2 .. the solve's or the launch's choice) as the
-  // scratch holds.
+  // The sweeps' z = P^-1 y of every block row stays in the scratch too when it
+  // fits next to two stage buffers (three vectors: a real and a complex
+  // right-hand side, or two real ones).  Then as many stage buffers (2 .. the
+  // solve's or the launch's choice) as the scratch holds.
   const bool staged = fac_bytes >= stage_total_bytes(bsz, esz, direct, bw, 2);
+  const long long zneed = (long long)(direct ? 3 : 2) * N * esz;
+  const bool zfit = fac_bytes >= stage_total_bytes(bsz, esz, direct, bw, 2) + zneed;
   const int want_bufs = d.sweep_bufs > 0 ? d.sweep_bufs : A.sweep_bufs;
   SolveStage SP;
   SP.nbuf = 2;
   while (SP.nbuf < min(want_bufs, kMaxStageBufs) &&
-         fac_bytes >= stage_total_bytes(bsz, esz, direct, bw, SP.nbuf + 1))
+         fac_bytes >= stage_total_bytes(bsz, esz, direct, bw, SP.nbuf + 1) + (zfit ? zneed : 0))
     ++SP.nbuf;
   SP.slot_r = stage_slot_bytes(bsz, esz);
   SP.slot_c = stage_slot_bytes(bsz, 2 * esz);
@@ -255,6 +264,11 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
   for (int q = 0; q < kMaxStageBufs; ++q)
     SP.buf[q] = reinterpret_cast<unsigned char*>(sbig) + size_t(min(q, SP.nbuf)) * sbytes;
   SP.ring = reinterpret_cast<void*>(SP.buf[0] + size_t(SP.nbuf) * sbytes);
+  SP.rhs_bulk = (bsz % 2) == 0;
+  SP.zbuf = zfit ? reinterpret_cast<void*>(reinterpret_cast<unsigned char*>(sbig) +
+                                          stage_total_bytes(bsz, esz, direct, bw, SP.nbuf))
+                 : nullptr;
+  SP.zcap = zfit ? int(zneed) : 0;
   SP.bar = S.pipe_bar;
   SP.err = &S.pipe_err;
   SP.wait_limit = d.stage_wait > 0 ? (long long)d.stage_wait : kBulkWaitLimit;
@@ -305,8 +319,8 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
     n_pass_r += nr > 0;
     n_pass_c += nc > 0;
     SolveSet<FT> Sv;
-    Sv.R = &LR;
-    Sv.Cf = &LC;
+    Sv.R = LR;
+    Sv.Cf = LC;
     Sv.xr[0] = xr0;
     Sv.xr[1] = xr1;
     Sv.zr[0] = vslot(C, RV_Z0);
@@ -444,13 +458,14 @@ __global__ void __launch_bounds__(FPE_RADAU_THREADS, 1) k_radau(RadauKernelArgs<
     }
     if (need_lu) {
       const long long t_f0 = clock64();
-      blu_assemble<FT>(O, LR, U1, 0.0, h);
-      if (direct) blu_assemble<Cx<FT>>(O, LC, ALPH, BETA, h);
+      blu_assemble_pair<FT>(O, LR, LC, direct, U1, ALPH, BETA, h);
       t_fasm += clock64() - t_f0;
       FT* scr_r = reinterpret_cast<FT*>(sbig);
       Cx<FT>* scr_c = reinterpret_cast<Cx<FT>*>(
           (reinterpret_cast<uintptr_t>(scr_r + scr_elems) + 15) & ~uintptr_t(15));
-      const bool fac_ok = blu_factor_pair<FT>(LR, direct ? &LC : nullptr, scr_r, scr_c, t_fsub);
+      const bool fac_ok =
+          fac_shared ? blu_factor_pair_smem<FT>(LR, LC, direct, dsmem_offset(scr_r), dsmem_offset(scr_c), t_fsub)
+                     : blu_factor_pair_gmem<FT>(LR, LC, direct, scr_r, scr_c, t_fsub);
       t_factor += clock64() - t_f0;
       if (!fac_ok) {  // a zero or non-finite pivot: no step can use these factors
         status = FPE_ERR_SINGULAR;
