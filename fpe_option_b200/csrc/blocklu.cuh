@@ -292,6 +292,13 @@ __device__ __forceinline__ Cx<T> finv(Cx<T> a) {
   const T d = a.re * a.re + a.im * a.im;
   return d != T(0) ? cmk(a.re / d, -a.im / d) : cmk(T(0), T(0));
 }
+// FP32: one reciprocal instead of two divisions (the pivot inverse is on the
+// Gauss-Jordan's serial path)
+__device__ __forceinline__ Cx<float> finv(Cx<float> a) {
+  const float d = a.re * a.re + a.im * a.im;
+  const float r = d != 0.f ? 1.f / d : 0.f;
+  return cmk(a.re * r, -a.im * r);
+}
 __device__ __forceinline__ double fmag(float a) { return fabs(double(a)); }
 __device__ __forceinline__ double fmag(double a) { return fabs(a); }
 template <typename T>
@@ -313,13 +320,12 @@ __device__ __forceinline__ double fmag(Cx<T> a) {
 //   EbT  bw x nvp x ldt   E_{i+1+r, i}, transposed
 //   LbT  bw x nvp x ldt   L_{i+1+r, i} = E P^-1, transposed (left operand of the Schur update)
 //   Ub   bw x nvp x nvp   U_{i, i+1+c}, row-major
-//   pbuf 2 x nvp          the published pivot row of the register Gauss-Jordan
 //   pinv nvp (inverse pivot of each column), then the pivot rows prow_of and
 //   their columns q_of (int)
 // --------------------------------------------------------------------------
 template <typename ET>
 struct FacScratch {
-  ET *aug, *Pi, *PiT, *EbT, *LbT, *Ub, *pbuf;
+  ET *aug, *Pi, *PiT, *EbT, *LbT, *Ub;
   ET* pinv;      // inverse pivot value of each column
   int* prow_of;  // pivot row of each column
   int* q_of;     // column whose pivot row is r
@@ -339,8 +345,7 @@ struct FacScratch {
     EbT = PiT + p * t;
     LbT = EbT + bw * p * t;
     Ub = LbT + bw * p * t;
-    pbuf = Ub + bw * p * p;
-    pinv = pbuf + 2 * p;
+    pinv = Ub + bw * p * p;
     prow_of = reinterpret_cast<int*>(pinv + p);
     q_of = prow_of + p;
     claim = q_of + p;
@@ -530,12 +535,33 @@ template <typename T>
 __device__ __forceinline__ float pmag(Cx<T> a) {
   return float(fabs(double(a.re)) + fabs(double(a.im)));
 }
+__device__ __forceinline__ float pmag(Cx<float> a) { return fabsf(a.re) + fabsf(a.im); }
 
 // Pivot key of row r: the magnitude's float bits above bit 7, then 127 - r,
 // so one unsigned max over the warp picks the largest magnitude and, among
 // equal keys, the lowest row.  Rows already pivotal have key 0.
 __device__ __forceinline__ unsigned pivot_key(float m, int r) {
   return (__float_as_uint(m) & ~127u) | unsigned(127 - r);
+}
+
+template <typename ET>
+struct IsF32Elem { static constexpr bool v = false; };
+template <>
+struct IsF32Elem<float> { static constexpr bool v = true; };
+template <>
+struct IsF32Elem<Cx<float>> { static constexpr bool v = true; };
+
+// One Gauss-Jordan update a - f p: fused multiply-adds for FP32 elements
+// (fewer instructions on the inversion's serial path), a rounded product then
+// a difference for FP64 ones.
+template <typename ET>
+__device__ __forceinline__ ET gj_elim(ET a, ET f, ET p) {
+  if constexpr (IsF32Elem<ET>::v) {
+    ffms(a, f, p);
+    return a;
+  } else {
+    return fsub(a, fmul(f, p));
+  }
 }
 
 // In-place Gauss-Jordan inversion of the staged pivot block by one warp, with
@@ -587,9 +613,9 @@ __device__ __forceinline__ bool fac_gj_warp(FacScratch<ET>& S) {
           rv[k] = row[l + k];
         }
 #pragma unroll
-        for (int k = 0; k < 8; ++k) row[l + k] = fsub(rv[k], fmul(f, pv[k]));
+        for (int k = 0; k < 8; ++k) row[l + k] = gj_elim(rv[k], f, pv[k]);
       }
-      for (; l < nv; ++l) row[l] = fsub(row[l], fmul(f, ap[l]));
+      for (; l < nv; ++l) row[l] = gj_elim(row[l], f, ap[l]);
       row[c] = fsub(fzero(ET()), f);
     };
     if (own0 && r0 != p) eliminate(a0);
@@ -601,85 +627,81 @@ __device__ __forceinline__ bool fac_gj_warp(FacScratch<ET>& S) {
   return ok;
 }
 
+// Lane-to-lane copy of a register element (the pivot row's broadcast).
+__device__ __forceinline__ float shfl_elem(float v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ Cx<float> shfl_elem(Cx<float> v, int src) {
+  return cmk(__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src));
+}
+
 // The same Gauss-Jordan inversion with each lane's row in registers (FP32
-// blocks of NV <= 32 columns): lane r keeps row r for the whole inversion, and
-// the pivot lane publishes its row each step through one of two alternating
-// shared rows (the next step writes the other, so one __syncwarp per step
-// orders a publication before its reads and after the previous-but-one
-// step's reads).  The row rotates left by one column per step, so the current
-// column is always element 0 and the loop body is one compiled step; after NV
-// steps the columns are back in order.  The pivot choice, the arithmetic of
-// each element and the bookkeeping are those of fac_gj_warp.
+// blocks of NV <= 32 columns): lane r keeps row r for the whole inversion,
+// and each step broadcasts the pivot row from its lane by shuffles (no
+// shared-memory round trip, no divergent stores).  The row rotates left by
+// four columns every four steps, so the current column is one of elements
+// 0..3 and the loop body is four compiled steps (register indices are
+// compile-time); after NV steps the columns are back in order.  The pivot
+// choice, the arithmetic of each element and the bookkeeping are those of
+// fac_gj_warp.
 template <typename ET, int NV>
-__device__ __noinline__ bool fac_gj_warp_reg(uint32_t aug_off, uint32_t pbuf_off, uint32_t pinv_off,
-                                              uint32_t prow_off, uint32_t qof_off) {
+__device__ __noinline__ bool fac_gj_warp_reg(uint32_t aug_off, uint32_t pinv_off, uint32_t prow_off,
+                                              uint32_t qof_off) {
   static_assert(NV <= 32 && NV % 4 == 0, "register rows of up to 32 columns, 16-byte chunks");
   // the scratch arrays, rebuilt from shared offsets so that their accesses are LDS / STS
-  struct {
-    ET *aug, *pbuf, *pinv;
-    int *prow_of, *q_of;
-  } S{reinterpret_cast<ET*>(fpe_dsmem + aug_off), reinterpret_cast<ET*>(fpe_dsmem + pbuf_off),
-      reinterpret_cast<ET*>(fpe_dsmem + pinv_off), reinterpret_cast<int*>(fpe_dsmem + prow_off),
-      reinterpret_cast<int*>(fpe_dsmem + qof_off)};
+  ET* const aug = reinterpret_cast<ET*>(fpe_dsmem + aug_off);
+  ET* const pinv = reinterpret_cast<ET*>(fpe_dsmem + pinv_off);
+  int* const prow_of = reinterpret_cast<int*>(fpe_dsmem + prow_off);
+  int* const q_of = reinterpret_cast<int*>(fpe_dsmem + qof_off);
   const int lane = threadIdx.x & 31, w1 = NV + 1;
   const bool own = lane < NV;
   ET row[NV];
 #pragma unroll
-  for (int l = 0; l < NV; ++l) row[l] = own ? S.aug[lane * w1 + l] : fzero(ET());
+  for (int l = 0; l < NV; ++l) row[l] = own ? aug[lane * w1 + l] : fzero(ET());
   bool used = false, ok = true;
 #pragma unroll 1
-  for (int c = 0; c < NV; ++c) {
-    const unsigned k = (own && !used) ? pivot_key(pmag(row[0]), lane) : 0u;
-    const unsigned kmax = __reduce_max_sync(0xffffffffu, k);
-    const int p = min(127 - int(kmax & 127u), NV - 1);  // an unused row always has a nonzero key
-    ET* pb = S.pbuf + (c & 1) * NV;
-    if (lane == p) {
+  for (int c0 = 0; c0 < NV; c0 += 4) {
 #pragma unroll
-      for (int l = 0; l < NV; ++l) pb[l] = row[l];
-    }
-    __syncwarp();
-    const ET pv = pb[0];
-    const float pm = pmag(pv);
-    ok &= (pm > 0.f) && (pm < CUDART_INF_F);
-    const ET inv = finv(pv);
-    if (lane == 0) {
-      S.prow_of[c] = p;
-      S.q_of[p] = c;
-      S.pinv[c] = inv;
-    }
-    if (lane == p) {
-      used = true;
-      row[0] = fone(ET());
-    } else if (own) {
-      const ET f = fmul(row[0], inv);
+    for (int u = 0; u < 4; ++u) {
+      const int c = c0 + u;
+      const unsigned k = (own && !used) ? pivot_key(pmag(row[u]), lane) : 0u;
+      const unsigned kmax = __reduce_max_sync(0xffffffffu, k);
+      const int p = min(127 - int(kmax & 127u), NV - 1);  // an unused row always has a nonzero key
+      const ET pv = shfl_elem(row[u], p);
+      ET q[NV];
 #pragma unroll
-      for (int l0 = 0; l0 < NV; l0 += 4) {
-        ET q[4];
-        vld<4>(pb + l0, q);
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (l0 + j > 0) row[l0 + j] = fsub(row[l0 + j], fmul(f, q[j]));
+      for (int l = 0; l < NV; ++l) q[l] = l == u ? pv : shfl_elem(row[l], p);
+      const float pm = pmag(pv);
+      ok &= (pm > 0.f) && (pm < CUDART_INF_F);
+      const ET inv = finv(pv);
+      if (lane == 0) {
+        prow_of[c] = p;
+        q_of[p] = c;
+        pinv[c] = inv;
       }
-      row[0] = fsub(fzero(ET()), f);
-    }
-    const ET t0 = row[0];
+      if (lane == p) {
+        used = true;
+        row[u] = fone(ET());
+      } else if (own) {
+        const ET f = fmul(row[u], inv);
 #pragma unroll
-    for (int l = 0; l + 1 < NV; ++l) row[l] = row[l + 1];
-    row[NV - 1] = t0;
+        for (int l = 0; l < NV; ++l)
+          if (l != u) row[l] = gj_elim(row[l], f, q[l]);
+        row[u] = fsub(fzero(ET()), f);
+      }
+    }
+    ET t[4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) t[l] = row[l];
+#pragma unroll
+    for (int l = 0; l + 4 < NV; ++l) row[l] = row[l + 4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) row[NV - 4 + l] = t[l];
   }
   if (own) {
 #pragma unroll
-    for (int l = 0; l < NV; ++l) S.aug[lane * w1 + l] = row[l];
+    for (int l = 0; l < NV; ++l) aug[lane * w1 + l] = row[l];
   }
   return ok;
 }
-
-template <typename ET>
-struct IsF32Elem { static constexpr bool v = false; };
-template <>
-struct IsF32Elem<float> { static constexpr bool v = true; };
-template <>
-struct IsF32Elem<Cx<float>> { static constexpr bool v = true; };
 
 // The pivot-block inverse: rows in registers for FP32 blocks of 8 to 32
 // columns (multiples of 4), rows in shared memory otherwise.
@@ -687,14 +709,14 @@ template <typename ET>
 __device__ __forceinline__ bool fac_gj(FacScratch<ET>& S) {
   if constexpr (IsF32Elem<ET>::v) {
     if (S.shared) {
-      const uint32_t a = dsmem_offset(S.aug), pb = dsmem_offset(S.pbuf), pi = dsmem_offset(S.pinv),
-                     pr = dsmem_offset(S.prow_of), qo = dsmem_offset(S.q_of);
+      const uint32_t a = dsmem_offset(S.aug), pi = dsmem_offset(S.pinv), pr = dsmem_offset(S.prow_of),
+                     qo = dsmem_offset(S.q_of);
       switch (S.nv) {
-        case 8: return fac_gj_warp_reg<ET, 8>(a, pb, pi, pr, qo);
-        case 12: return fac_gj_warp_reg<ET, 12>(a, pb, pi, pr, qo);
-        case 16: return fac_gj_warp_reg<ET, 16>(a, pb, pi, pr, qo);
-        case 24: return fac_gj_warp_reg<ET, 24>(a, pb, pi, pr, qo);
-        case 32: return fac_gj_warp_reg<ET, 32>(a, pb, pi, pr, qo);
+        case 8: return fac_gj_warp_reg<ET, 8>(a, pi, pr, qo);
+        case 12: return fac_gj_warp_reg<ET, 12>(a, pi, pr, qo);
+        case 16: return fac_gj_warp_reg<ET, 16>(a, pi, pr, qo);
+        case 24: return fac_gj_warp_reg<ET, 24>(a, pi, pr, qo);
+        case 32: return fac_gj_warp_reg<ET, 32>(a, pi, pr, qo);
         default: break;
       }
     }

@@ -143,7 +143,7 @@ FPE_HD int fpe_block_stride(int b) { return (b * b + 3) & ~3; }
 FPE_HD int fpe_fac_scratch_elems(int b, int bw = 3) {
   const int p = fpe_fac_nvp(b), t = p + 4;
   const int aug = (b * (b + 1) + 3) & ~3;
-  return aug + p * p + p * t + bw * p * t + bw * p * t + bw * p * p + 2 * p + 3 * p + (3 * p + 4);
+  return aug + p * p + p * t + bw * p * t + bw * p * t + bw * p * p + 3 * p + (3 * p + 4);
 }
 
 // Shared memory of the IC projection's ADMM (bytes): eigenvector matrices
