@@ -311,7 +311,8 @@ __device__ __forceinline__ double fmag(Cx<T> a) {
 //
 // Blocks (b x b; b is called nv inside the scratch) are staged with a padded
 // width nvp = b rounded up to 4 so that every tile operand is a 16-byte vector
-// load.  GEMM left operands are stored transposed (k-major, row stride
+// load and the blocks hold a whole number of register tiles (the padding is
+// never written: it only meets tile rows and columns that are not stored).  GEMM left operands are stored transposed (k-major, row stride
 // ldt = nvp + 4: the transposed staging writes spread over 8 banks), right
 // operands row-major (stride nvp).
 //   aug  nv x (nv + 1)    in-place Gauss-Jordan array of the pivot block
@@ -362,7 +363,10 @@ struct TileM { static constexpr int v = 4; };
 #endif
 template <typename T>
 struct TileM<Cx<T>> { static constexpr int v = FPE_CTILE_M; };
-constexpr int kTileN = 4;
+// Tile width per element type (4 columns; the scratch pads blocks to a
+// multiple of the widest tile).
+template <typename ET>
+struct TileN { static constexpr int v = 4; };
 
 // Vector loads/stores of K consecutive elements from 16-byte aligned shared memory.
 template <int K>
@@ -426,6 +430,18 @@ __device__ __forceinline__ void vst16(Cx<double>* p, const Cx<double> (&v)[2]) {
   reinterpret_cast<double2*>(p)[0] = make_double2(v[0].re, v[0].im);
   reinterpret_cast<double2*>(p)[1] = make_double2(v[1].re, v[1].im);
 }
+// K consecutive elements (K a multiple of 4) to a 16-byte aligned address.
+template <typename ET, int K>
+__device__ __forceinline__ void vstn(ET* p, const ET (&v)[K]) {
+  static_assert(K % 4 == 0, "runs of 4 elements");
+#pragma unroll
+  for (int q = 0; q < K; q += 4) {
+    ET w[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) w[r] = v[q + r];
+    vst16(p + q, w);
+  }
+}
 
 __device__ __forceinline__ void ffms(float& a, float x, float y) { a = fmaf(-x, y, a); }
 __device__ __forceinline__ void ffms(double& a, double x, double y) { a = fma(-x, y, a); }
@@ -440,11 +456,11 @@ __device__ __forceinline__ void ffms(Cx<T>& a, Cx<T> x, Cx<T> y) {
 // acc (+)= sum_k AT[k][j0 + m] B[k][l0 + n], k < K  (SUB: acc -= ...)
 template <typename ET, bool SUB>
 __device__ __forceinline__ void tile_mm(const ET* AT, int lda, const ET* B, int ldb, int K, int j0, int l0,
-                                        ET (&acc)[TileM<ET>::v][kTileN]) {
-  constexpr int TM = TileM<ET>::v;
+                                        ET (&acc)[TileM<ET>::v][TileN<ET>::v]) {
+  constexpr int TM = TileM<ET>::v, kTileN = TileN<ET>::v;
   const ET* pa = AT + j0;
   const ET* pb = B + l0;
-#pragma unroll 2
+#pragma unroll 4
   for (int k = 0; k < K; ++k) {
     ET a[TM], b[kTileN];
     vld<TM>(pa + k * lda, a);
@@ -752,55 +768,62 @@ __device__ __forceinline__ void fac_extract(const BlockLU<ET>& L, FacScratch<ET>
 // numbered with the row index j varying fastest, so that a lane's TM rows of
 // one output column are contiguous in the transposed storage: one vector
 // store each, and a warp's stores cover contiguous memory.
+// Tile tt of job `job` (job < nr: L_job; else W_{job - nr}).
 template <typename ET>
-__device__ __forceinline__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
-  constexpr int TM = TileM<ET>::v;
+__device__ __forceinline__ void fac_lw_tile(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, int job, int tt) {
+  constexpr int TM = TileM<ET>::v, kTileN = TileN<ET>::v;
   const int nv = S.nv, p = S.nvp, t = S.ldt;
-  const int tr = p / TM, tc = p / kTileN, ntile = tr * tc;
+  const int tr = p / TM;
   const bool vec = ((nv * int(sizeof(ET))) & 15) == 0 && ((L.bs * sizeof(ET)) & 15) == 0 &&
                    (reinterpret_cast<uintptr_t>(L.F) & 15) == 0;
-  for (int q = threadIdx.x; q < 2 * nr * ntile; q += blockDim.x) {
-    const int job = q / ntile, tt = q - job * ntile;
-    const int l0 = (tt / tr) * kTileN, j0 = (tt - (tt / tr) * tr) * TM;
-    ET acc[TM][kTileN];
+  const int l0 = (tt / tr) * kTileN, j0 = (tt - (tt / tr) * tr) * TM;
+  ET acc[TM][kTileN];
 #pragma unroll
-    for (int m = 0; m < TM; ++m)
+  for (int m = 0; m < TM; ++m)
 #pragma unroll
-      for (int n = 0; n < kTileN; ++n) acc[m][n] = fzero(ET());
-    ET* dst;
-    if (job < nr) {
-      tile_mm<ET, false>(S.EbT + job * p * t, t, S.Pi, p, nv, j0, l0, acc);
-      dst = L.blk(i + 1 + job, L.bw - 1 - job);
-      ET* lt = S.LbT + job * p * t;
+    for (int n = 0; n < kTileN; ++n) acc[m][n] = fzero(ET());
+  ET* dst;
+  if (job < nr) {
+    tile_mm<ET, false>(S.EbT + job * p * t, t, S.Pi, p, nv, j0, l0, acc);
+    dst = L.blk(i + 1 + job, L.bw - 1 - job);
+    ET* lt = S.LbT + job * p * t;
 #pragma unroll
-      for (int n = 0; n < kTileN; ++n) {
+    for (int n = 0; n < kTileN; ++n) {
+      ET col[TM];
+#pragma unroll
+      for (int m = 0; m < TM; ++m) col[m] = acc[m][n];
+      vst<ET, TM>(lt + (l0 + n) * t + j0, col);
+    }
+  } else {
+    const int cc = job - nr;
+    tile_mm<ET, false>(S.PiT, t, S.Ub + cc * p * p, p, nv, j0, l0, acc);
+    dst = L.blk(i, L.bw + 1 + cc);
+  }
+  if (vec && j0 + TM <= nv) {
+#pragma unroll
+    for (int n = 0; n < kTileN; ++n) {
+      if (l0 + n < nv) {
         ET col[TM];
 #pragma unroll
         for (int m = 0; m < TM; ++m) col[m] = acc[m][n];
-        vst<ET, TM>(lt + (l0 + n) * t + j0, col);
+        vst16(dst + (l0 + n) * nv + j0, col);
       }
-    } else {
-      const int cc = job - nr;
-      tile_mm<ET, false>(S.PiT, t, S.Ub + cc * p * p, p, nv, j0, l0, acc);
-      dst = L.blk(i, L.bw + 1 + cc);
     }
-    if (vec && j0 + TM <= nv) {
+  } else {
 #pragma unroll
-      for (int n = 0; n < kTileN; ++n) {
-        if (l0 + n < nv) {
-          ET col[TM];
+    for (int m = 0; m < TM; ++m)
 #pragma unroll
-          for (int m = 0; m < TM; ++m) col[m] = acc[m][n];
-          vst16(dst + (l0 + n) * nv + j0, col);
-        }
-      }
-    } else {
-#pragma unroll
-      for (int m = 0; m < TM; ++m)
-#pragma unroll
-        for (int n = 0; n < kTileN; ++n)
-          if (j0 + m < nv && l0 + n < nv) dst[(l0 + n) * nv + j0 + m] = acc[m][n];
-    }
+      for (int n = 0; n < kTileN; ++n)
+        if (j0 + m < nv && l0 + n < nv) dst[(l0 + n) * nv + j0 + m] = acc[m][n];
+  }
+}
+
+template <typename ET>
+__device__ __forceinline__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr) {
+  const int ntile = (S.nvp / TileM<ET>::v) * (S.nvp / TileN<ET>::v);
+  for (int q = threadIdx.x; q < 2 * nr * ntile; q += blockDim.x) {
+    const int job = q / ntile;
+    fac_lw_tile<ET>(L, S, i, nr, job, q - job * ntile);
   }
 }
 
@@ -812,7 +835,7 @@ __device__ __forceinline__ void fac_lw(const BlockLU<ET>& L, FacScratch<ET>& S, 
 // there, and the factor storage of that block receives its inverse.
 template <typename ET>
 __device__ __forceinline__ int fac_tiles(const FacScratch<ET>& S) {
-  return (S.nvp / TileM<ET>::v) * (S.nvp / kTileN);
+  return (S.nvp / TileM<ET>::v) * (S.nvp / TileN<ET>::v);
 }
 
 // Tile q of the Schur jobs job_lo, job_lo + 1, ... (q = job offset x tiles per
@@ -820,7 +843,7 @@ __device__ __forceinline__ int fac_tiles(const FacScratch<ET>& S) {
 template <typename ET, bool TO_AUG>
 __device__ __forceinline__ void fac_update_tile(const BlockLU<ET>& L, FacScratch<ET>& S, int i, int nr, int job_lo,
                                                 int q) {
-  constexpr int TM = TileM<ET>::v;
+  constexpr int TM = TileM<ET>::v, kTileN = TileN<ET>::v;
   const int nv = S.nv, p = S.nvp, t = S.ldt;
   const int tc = p / kTileN, ntile = fac_tiles(S);
   {
@@ -829,18 +852,48 @@ __device__ __forceinline__ void fac_update_tile(const BlockLU<ET>& L, FacScratch
     const int rr = job / nr, cc = job - rr * nr;
     ET* E = L.blk(i + 1 + rr, cc - rr + L.bw);
     ET acc[TM][kTileN];
+    if constexpr (IsF32Elem<ET>::v) {
+      // FP32: the products accumulate from zero and the target tile (global
+      // memory, written by the previous block row's updates) is subtracted
+      // at the end, so its loads are in flight while the products run
+      // instead of holding up the first one
+      ET e[TM][kTileN];
+      const bool vec = (nv & 3) == 0 && l0 + kTileN <= nv;  // rows of the tile are 16-byte aligned runs
 #pragma unroll
-    for (int m = 0; m < TM; ++m)
+      for (int m = 0; m < TM; ++m) {
+        if (vec && j0 + m < nv) {
+          vld<kTileN>(E + (j0 + m) * nv + l0, e[m]);
+        } else {
 #pragma unroll
-      for (int n = 0; n < kTileN; ++n)
-        acc[m][n] = (j0 + m < nv && l0 + n < nv) ? E[(j0 + m) * nv + l0 + n] : fzero(ET());
-    tile_mm<ET, true>(S.LbT + rr * p * t, t, S.Ub + cc * p * p, p, nv, j0, l0, acc);
+          for (int n = 0; n < kTileN; ++n)
+            e[m][n] = (j0 + m < nv && l0 + n < nv) ? E[(j0 + m) * nv + l0 + n] : fzero(ET());
+        }
+#pragma unroll
+        for (int n = 0; n < kTileN; ++n) acc[m][n] = fzero(ET());
+      }
+      tile_mm<ET, false>(S.LbT + rr * p * t, t, S.Ub + cc * p * p, p, nv, j0, l0, acc);
+#pragma unroll
+      for (int m = 0; m < TM; ++m)
+#pragma unroll
+        for (int n = 0; n < kTileN; ++n) acc[m][n] = fsub(e[m][n], acc[m][n]);
+    } else {
+#pragma unroll
+      for (int m = 0; m < TM; ++m)
+#pragma unroll
+        for (int n = 0; n < kTileN; ++n)
+          acc[m][n] = (j0 + m < nv && l0 + n < nv) ? E[(j0 + m) * nv + l0 + n] : fzero(ET());
+      tile_mm<ET, true>(S.LbT + rr * p * t, t, S.Ub + cc * p * p, p, nv, j0, l0, acc);
+    }
     if constexpr (TO_AUG) {
 #pragma unroll
       for (int m = 0; m < TM; ++m)
 #pragma unroll
         for (int n = 0; n < kTileN; ++n)
           if (j0 + m < nv && l0 + n < nv) S.aug[(j0 + m) * S.w1 + l0 + n] = acc[m][n];
+    } else if ((nv & 3) == 0 && l0 + kTileN <= nv) {
+#pragma unroll
+      for (int m = 0; m < TM; ++m)
+        if (j0 + m < nv) vstn(E + (j0 + m) * nv + l0, acc[m]);
     } else {
 #pragma unroll
       for (int m = 0; m < TM; ++m)
@@ -857,26 +910,33 @@ __device__ __forceinline__ void fac_update(const BlockLU<ET>& L, FacScratch<ET>&
   for (int q = lt; q < (job_hi - job_lo) * fac_tiles(S); q += nt) fac_update_tile<ET, TO_AUG>(L, S, i, nr, job_lo, q);
 }
 
-// Schur updates 1 .. nr^2 - 1 of both systems (real tiles first), claimed 32
-// tiles at a time per warp from a shared counter, so that the warps which
-// finish their pivot inverse early take their share of the products.
+// Schur updates 1 .. nr^2 - 1 of both systems, claimed 32 tiles at a time
+// per warp, so that the warps which finish their pivot inverse early take
+// their share of the products: the complex tiles first (counter ctr[0]), then
+// the real ones (ctr[1], four times less work a tile, which evens out the
+// warps' finishing times).  One loop per element type keeps each loop's
+// registers to one tile shape.
 template <typename FT>
 __device__ __forceinline__ void fac_update_claim(const BlockLU<FT>& LR, FacScratch<FT>& SR, const BlockLU<Cx<FT>>* LC,
                                  FacScratch<Cx<FT>>& SC, int i, int nr, int* ctr) {
   const int lane = threadIdx.x & 31;
-  const int nr_tiles = (nr * nr - 1) * fac_tiles(SR);
-  const int total = nr_tiles + (LC ? (nr * nr - 1) * fac_tiles(SC) : 0);
+  if (LC) {
+    const int total = (nr * nr - 1) * fac_tiles(SC);
+    for (;;) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(ctr, 32);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= total) break;
+      if (base + lane < total) fac_update_tile<Cx<FT>, false>(*LC, SC, i, nr, 1, base + lane);
+    }
+  }
+  const int total = (nr * nr - 1) * fac_tiles(SR);
   for (;;) {
     int base = 0;
-    if (lane == 0) base = atomicAdd(ctr, 32);
+    if (lane == 0) base = atomicAdd(ctr + 1, 32);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
-    const int q = base + lane;
-    if (q < nr_tiles) {
-      fac_update_tile<FT, false>(LR, SR, i, nr, 1, q);
-    } else if (q < total) {
-      fac_update_tile<Cx<FT>, false>(*LC, SC, i, nr, 1, q - nr_tiles);
-    }
+    if (base + lane < total) fac_update_tile<FT, false>(LR, SR, i, nr, 1, base + lane);
   }
 }
 
@@ -939,7 +999,10 @@ __device__ __forceinline__ bool blu_factor_pair(const BlockLU<FT>& LR, const Blo
           SC.prow_of[r] = r;
         }
       }
-      if (threadIdx.x == 0) *SR.claim = 0;
+      if (threadIdx.x == 0) {
+        SR.claim[0] = 0;
+        SR.claim[1] = 0;
+      }
       __syncthreads();
       const long long t3 = clock64();
       tc1 += t3 - t2;

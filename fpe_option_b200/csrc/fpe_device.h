@@ -131,10 +131,10 @@ FPE_HD int fpe_blk_bw(int m) { return 4 * m - 1; }
 
 // Stage-factorization scratch of one system, in elements, for block size b
 // and bw off-diagonal blocks: the pivot block's Gauss-Jordan array
-// b x (b + 1), then blocks padded to p = b rounded up to 4 (row-major p x p,
-// transposed p x (p + 4)): P^-1 both ways, bw transposed E and L blocks, bw U
-// blocks, two pivot-row buffers of p, and the pivot bookkeeping (with room to
-// spare).
+// b x (b + 1), then blocks padded to p = b rounded up to 4, a whole number
+// of register tiles (row-major p x p, transposed p x (p + 4)): P^-1 both
+// ways, bw transposed E and L blocks, bw U blocks, and the pivot bookkeeping
+// (with room to spare).
 FPE_HD int fpe_fac_nvp(int nv) { return (nv + 3) & ~3; }
 // Element stride between the b x b blocks of a stored stage factor: b^2
 // rounded up to 4, so every block starts and ends on a 16-byte boundary and
