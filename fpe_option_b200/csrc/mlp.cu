@@ -7,16 +7,21 @@
 // activations and gradients, written by the producing epilogues, so that the
 // weight gradients are K-major products over the batch as well.
 //
-// One CTA of 128 threads computes a 128 x N tile (N <= 256): K is staged in
-// 64-wide chunks into two shared-memory buffers in the canonical no-swizzle
-// K-major layout (8-row x 16-byte core matrices), one thread issues
-// tcgen05.mma (M = 128, N, K = 16) into a TMEM accumulator and commits to an
-// mbarrier, the next chunk loads while the MMAs run, and the epilogue reads
-// the accumulator back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31,
-// i.e. tile rows) and applies bias / SiLU / SiLU' before storing.
+// Products with K a multiple of 64 run in a persistent kernel (k_gemm_bf16_tma,
+// one CTA per SM): TMA loads 64-wide K chunks of A and B in the 128-byte
+// swizzled layout into a four-stage mbarrier pipeline, one thread issues
+// tcgen05.mma (M = 128, N <= 256, K = 16) into one of two TMEM accumulators,
+// and four epilogue warps drain the other accumulator (tcgen05.ld, bias /
+// SiLU / SiLU', stores) under the next tile's MMAs.  The remaining products
+// (K = 16 input layers, split-K weight gradients) use k_gemm_bf16_tc: one CTA
+// per 128 x N tile, K staged by cp.async into two buffers in the canonical
+// no-swizzle K-major layout, the next chunk loading while the MMAs run.  In
+// both, warp w reads TMEM lanes 32 (w % 4) .. + 31, the tile's rows.
 //
 // Adam follows the reference update rule (src/nn/adam.mojo:31-64).
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -110,7 +115,23 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + __expf(-z)); }
+// The same load without its completion wait (several loads, then one
+// tmem_wait_ld, before the registers are read).
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 1 / (1 + e^-z) with the hardware exponential and reciprocal (a few ulp; the
+// network's activations are rounded to BF16 anyway), branch-free so that the
+// epilogues' elements interleave.  z is clamped at -80 so that 1 + e^-z stays
+// below 2^126, where the fast division is exact to its stated error.
+__device__ __forceinline__ float sigmoidf_(float z) { return __fdividef(1.0f, 1.0f + __expf(-fmaxf(z, -80.0f))); }
 
 // ---- the product kernel --------------------------------------------------------
 enum Epi : int {
@@ -141,6 +162,60 @@ struct GemmParams {
   int atomic;  // EPI_F32: accumulate into Cf with atomicAdd (Cf zeroed by the caller)
   int* err;
 };
+
+// Epilogue of 16 accumulator columns gn .. gn + 15 of output row gm.
+// b: the 16 columns' biases (zeros without a bias).
+__device__ __forceinline__ void epilogue16(const GemmParams& P, const float (&b)[16], int gm, int gn, float (&v)[16]) {
+  if (P.epi == EPI_F32) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      float z = v[j] + b[j];
+      if (P.act) z = z * sigmoidf_(z);
+      v[j] = z;
+    }
+  } else if (P.epi == EPI_BIAS_SILU) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] += b[j];
+  } else {
+    const float* zr = P.zin + size_t(gm) * P.ldz + gn;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const float z = zr[j], s = sigmoidf_(z);
+      v[j] *= s * (1.0f + z * (1.0f - s));
+    }
+  }
+  if (P.Cf && P.atomic) {
+    float* d = P.Cf + size_t(gm) * P.ldcf + gn;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) atomicAdd(d + j, v[j]);
+  } else if (P.Cf) {
+    float4* d = reinterpret_cast<float4*>(P.Cf + size_t(gm) * P.ldcf + gn);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  }
+  if (P.Cb || P.CbT) {
+    __align__(16) __nv_bfloat162 h2[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float x0 = v[2 * j], x1 = v[2 * j + 1];
+      if (P.epi == EPI_BIAS_SILU) {
+        x0 *= sigmoidf_(x0);
+        x1 *= sigmoidf_(x1);
+      }
+      h2[j] = __floats2bfloat162_rn(x0, x1);  // one packed conversion per pair
+    }
+    const bf16* h = reinterpret_cast<const bf16*>(h2);
+    if (P.Cb) {
+      uint4* d = reinterpret_cast<uint4*>(P.Cb + size_t(gm) * P.ldcb + gn);
+      d[0] = *reinterpret_cast<const uint4*>(&h[0]);
+      d[1] = *reinterpret_cast<const uint4*>(&h[8]);
+    }
+    if (P.CbT) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) P.CbT[size_t(gn + j) * P.ldcbt + gm] = h[j];
+    }
+  }
+}
 
 // Stage rows [row0, row0 + rows) x K [k0, k0 + kc) of a K-contiguous BF16
 // matrix into the canonical layout: core matrix (row / 8, k / 8) at
@@ -245,51 +320,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
     for (int c = 16 * half; c < Nt; c += 32) {
       float v[16];
       tmem_ld16(trow + uint32_t(c), v);
-      const int gn = n0 + c;
-      if (P.epi == EPI_F32) {
+      float b[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          float z = v[j] + (P.bias ? P.bias[gn + j] : 0.0f);
-          if (P.act) z = z * sigmoidf_(z);
-          v[j] = z;
-        }
-      } else if (P.epi == EPI_BIAS_SILU) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] += P.bias ? P.bias[gn + j] : 0.0f;
-      } else {
-        const float* zr = P.zin + size_t(gm) * P.ldz + gn;
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const float z = zr[j], s = sigmoidf_(z);
-          v[j] *= s * (1.0f + z * (1.0f - s));
-        }
-      }
-      if (P.Cf && P.atomic) {
-        float* d = P.Cf + size_t(gm) * P.ldcf + gn;
-#pragma unroll
-        for (int j = 0; j < 16; ++j) atomicAdd(d + j, v[j]);
-      } else if (P.Cf) {
-        float4* d = reinterpret_cast<float4*>(P.Cf + size_t(gm) * P.ldcf + gn);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-      }
-      if (P.Cb || P.CbT) {
-        bf16 h[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const float x = P.epi == EPI_BIAS_SILU ? v[j] * sigmoidf_(v[j]) : v[j];
-          h[j] = __float2bfloat16_rn(x);
-        }
-        if (P.Cb) {
-          uint4* d = reinterpret_cast<uint4*>(P.Cb + size_t(gm) * P.ldcb + gn);
-          d[0] = *reinterpret_cast<const uint4*>(&h[0]);
-          d[1] = *reinterpret_cast<const uint4*>(&h[8]);
-        }
-        if (P.CbT) {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) P.CbT[size_t(gn + j) * P.ldcbt + gm] = h[j];
-        }
-      }
+      for (int j = 0; j < 16; ++j) b[j] = P.bias ? P.bias[n0 + c + j] : 0.0f;
+      epilogue16(P, b, gm, n0 + c, v);
     }
   } else if (!ok && tid == 0 && P.err) {
     atomicExch(P.err, 1);
@@ -297,6 +331,243 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, ncols);
+  }
+}
+
+// ---- persistent product with TMA staging ------------------------------------------
+// C = A B^T for M a multiple of 128, K a multiple of 64 and N-tiles of up to
+// 256 columns (a multiple of 16): one CTA per SM loops over the 128 x tn
+// output tiles, with three roles:
+//   warp 0 (one lane): TMA loads of the A and B K-chunks (64 BF16 = one
+//     128-byte swizzle row per matrix row) into kPStages shared-memory
+//     stages, each completing on its "full" mbarrier; a stage is refilled
+//     once its "empty" barrier says that the MMAs reading it are done;
+//   warp 1 (one lane): tcgen05.mma of each chunk into one of two TMEM
+//     accumulators, tcgen05.commit to the stage's "empty" barrier, and after a
+//     tile's last chunk to the accumulator's "full" barrier;
+//   warps 2..17: the epilogue of a finished accumulator (warp w reads TMEM
+//     lanes 32 (w % 4) .. + 31, the four warps of a lane quarter take turns
+//     at 16-column chunks), then an arrival on its "empty" barrier;
+// so the loads of later chunks, the MMAs of tile i + 1 and the epilogue of
+// tile i overlap.  Every wait is bounded: a wait that gives up sets *P.err and
+// ends the CTA's loop, and the copies and MMAs already issued are waited out
+// before the TMEM is released.  The tensor maps describe this GPU's own
+// operands only, and no load is multicast.
+constexpr int kPStages = 4;
+constexpr int kPThreads = 576;  // TMA warp, MMA warp, sixteen epilogue warps
+constexpr int kPStageA = kTileM * 128;  // 128 rows x 64 BF16
+constexpr int kPSmemBytes = kPStages * (kPStageA + kTileN * 128) + 1024;  // + alignment of the swizzle atoms
+
+// Shared-memory matrix descriptor of a K-major operand in the 128-byte
+// swizzled layout that TMA writes (rows of 128 bytes, 8-row groups 1024 bytes
+// apart): start address >> 4, stride byte offset 1024 >> 4, version 1,
+// layout type 2 (128-byte swizzle).  The leading byte offset is unused for
+// this layout.  An MMA step of K = 16 advances the start address by 32 bytes
+// inside the swizzle row.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= uint64_t((saddr >> 4) & 0x3FFFu);
+  d |= uint64_t(1) << 16;
+  d |= uint64_t(1024 >> 4) << 32;
+  d |= uint64_t(1) << 46;
+  d |= uint64_t(2) << 61;
+  return d;
+}
+
+// Tile (x = K offset in elements, y = row) of a 2-D tensor map into shared
+// memory, completing on bar.  x is a multiple of 64: 128 bytes.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__global__ void __launch_bounds__(kPThreads, 1)
+    k_gemm_bf16_tma(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                    GemmParams P) {
+  extern __shared__ __align__(1024) unsigned char psmem[];
+  __shared__ unsigned long long full[kPStages], empty[kPStages], accf[2], acce[2], done, bfull;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int give_up;  // a bounded wait gave up: every role leaves its loop
+  __shared__ float sbias[kTileN * 4];  // the biases of up to four N-tiles
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t base = (smem_u32(psmem) + 1023u) & ~1023u;  // swizzle atoms are 1024-byte aligned
+  const int BN = P.tn;
+  const int tiles_m = P.M / kTileM, ntiles = tiles_m * ((P.N + BN - 1) / BN);
+  const int nk = P.K / kChunkK;
+  uint32_t acc_cols = 32;
+  while (int(acc_cols) < BN) acc_cols <<= 1;
+  const uint32_t ncols = 2 * acc_cols;  // two accumulators
+  // With one N-tile whose B fits the stages' B area (K <= 256 at N = 256), B
+  // stays resident: its nk chunks are loaded once, at the start, and the
+  // stages carry A alone (a sixth of the bytes per tile at K = N = 256).
+  const bool bres = P.N <= BN && uint32_t(nk) * uint32_t(BN) * 128u <= uint32_t(kPStages * kTileN * 128);
+  const uint32_t bchunk = uint32_t(BN) * 128u;  // bytes of one B chunk
+  const uint32_t stage_bytes = bres ? uint32_t(kPStageA) : uint32_t(kPStageA) + bchunk;
+  const uint32_t abase = bres ? base + uint32_t(kPStages * kTileN * 128) : base;  // stage 0
+  if (warp == 1) tmem_alloc(&tmem_slot, ncols);
+  if (tid == 0) {
+    for (int s = 0; s < kPStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&accf[a], 1);
+      mbar_init(&acce[a], kPThreads - 64);
+    }
+    mbar_init(&done, 1);
+    mbar_init(&bfull, 1);
+    give_up = 0;
+    mbar_init_fence();
+  }
+  const bool bias_sh = P.bias && P.N <= kTileN * 4;
+  if (bias_sh)
+    for (int j = tid; j < P.N; j += blockDim.x) sbias[j] = P.bias[j];
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  // the 16 biases of columns n .. n + 15 (shared-memory loads when the copy exists)
+  auto bias16 = [&](int n, float (&b)[16]) {
+    if (bias_sh) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) b[j] = sbias[n + j];
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) b[j] = P.bias ? P.bias[n + j] : 0.0f;
+    }
+  };
+  auto fail = [&]() {
+    give_up = 1;
+    if (P.err) atomicExch(P.err, 1);
+  };
+  if (warp == 0) {
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t ph = 0, pend = 0, pend_ph = 0;  // stages with a load in flight, and its phase parity
+      const bool any = int(blockIdx.x) < ntiles;
+      if (bres && any) {
+        mbar_arrive_expect_tx(&bfull, uint32_t(nk) * bchunk);
+        for (int kc = 0; kc < nk; ++kc)
+          tma_load_2d(base + uint32_t(kc) * bchunk, &mapB, kc * kChunkK, 0, smem_u32(&bfull));
+      }
+      for (int t = blockIdx.x; t < ntiles && !give_up; t += gridDim.x) {
+        const int m0 = (t % tiles_m) * kTileM, n0 = (t / tiles_m) * BN;
+        for (int kc = 0; kc < nk; ++kc) {
+          // a fresh barrier counts as having completed the phase before its first
+          if (!mbar_wait_bounded(&empty[stage], ph ^ 1u, kBulkWaitLimit)) {
+            fail();
+            break;
+          }
+          const uint32_t sa = abase + uint32_t(stage) * stage_bytes;
+          mbar_arrive_expect_tx(&full[stage], stage_bytes);
+          tma_load_2d(sa, &mapA, kc * kChunkK, m0, smem_u32(&full[stage]));
+          if (!bres) tma_load_2d(sa + kPStageA, &mapB, kc * kChunkK, n0, smem_u32(&full[stage]));
+          pend |= 1u << stage;
+          pend_ph = (pend_ph & ~(1u << stage)) | (ph << stage);
+          if (++stage == kPStages) {
+            stage = 0;
+            ph ^= 1u;
+          }
+        }
+      }
+      // the loads this thread issued have all landed before the CTA ends
+      for (int s = 0; s < kPStages; ++s)
+        if ((pend >> s) & 1u) mbar_wait_bounded(&full[s], (pend_ph >> s) & 1u, kBulkWaitLimit);
+      if (bres && any) mbar_wait_bounded(&bfull, 0, kBulkWaitLimit);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int stage = 0, acc = 0;
+      uint32_t ph = 0, aph = 0;
+      const uint32_t idesc = umma_idesc_bf16(kTileM, BN);
+      if (bres && int(blockIdx.x) < ntiles && !mbar_wait_bounded(&bfull, 0, kBulkWaitLimit)) fail();
+      for (int t = blockIdx.x; t < ntiles && !give_up; t += gridDim.x) {
+        if (!mbar_wait_bounded(&acce[acc], aph ^ 1u, kBulkWaitLimit)) {
+          fail();
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + uint32_t(acc) * acc_cols;
+        bool ok = true;
+        for (int kc = 0; kc < nk; ++kc) {
+          if (!mbar_wait_bounded(&full[stage], ph, kBulkWaitLimit)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = abase + uint32_t(stage) * stage_bytes;
+          const uint32_t sb = bres ? base + uint32_t(kc) * bchunk : sa + kPStageA;
+#pragma unroll
+          for (int s = 0; s < kChunkK / 16; ++s)
+            umma_bf16(d, umma_desc_sw128(sa + 32u * s), umma_desc_sw128(sb + 32u * s), idesc,
+                      (kc > 0 || s > 0) ? 1u : 0u);
+          umma_commit(&empty[stage]);  // the stage is free once these MMAs are done
+          if (++stage == kPStages) {
+            stage = 0;
+            ph ^= 1u;
+          }
+        }
+        if (!ok) {
+          fail();
+          break;
+        }
+        umma_commit(&accf[acc]);  // the accumulator is complete once every MMA above is
+        acc ^= 1;
+        if (acc == 0) aph ^= 1u;
+      }
+      // every MMA this thread issued has finished before the TMEM is released
+      umma_commit(&done);
+      mbar_wait_bounded(&done, 0, kBulkWaitLimit);
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, the tile's rows,
+    // and the 16-column chunks h, h + 4, h + 8, ... (h = (w - 2) / 4), two
+    // chunks per completion wait
+    const int quarter = warp & 3, row = 32 * quarter + lane, h = (warp - 2) >> 2;
+    int acc = 0;
+    uint32_t aph = 0;
+    // the warp's decisions are uniform: tcgen05.ld is warp-collective
+    for (int t = blockIdx.x; t < ntiles && !__any_sync(0xffffffffu, give_up != 0); t += gridDim.x) {
+      const int m0 = (t % tiles_m) * kTileM, n0 = (t / tiles_m) * BN;
+      const int Nt = min(BN, P.N - n0);
+      if (!__all_sync(0xffffffffu, mbar_wait_bounded(&accf[acc], aph, kBulkWaitLimit))) {
+        fail();
+        break;
+      }
+      tc_fence_after();
+      const uint32_t trow = tmem + (uint32_t(32 * quarter) << 16) + uint32_t(acc) * acc_cols;
+      for (int c = 16 * h; c < Nt; c += 128) {
+        uint32_t r0[16], r1[16];
+        const bool two = c + 64 < Nt;  // uniform in the warp
+        tmem_ld16_async(trow + uint32_t(c), r0);
+        if (two) tmem_ld16_async(trow + uint32_t(c + 64), r1);
+        tmem_wait_ld();
+        float v[16], b[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r0[j]);
+        bias16(n0 + c, b);
+        epilogue16(P, b, m0 + row, n0 + c, v);
+        if (two) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r1[j]);
+          bias16(n0 + c + 64, b);
+          epilogue16(P, b, m0 + row, n0 + c + 64, v);
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acce[acc]);
+      acc ^= 1;
+      if (acc == 0) aph ^= 1u;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
     tc_fence_after();
     tmem_dealloc(tmem, ncols);
   }
@@ -470,6 +741,12 @@ using fpe::mlp::bf16;
 struct MlpCtx {
   bool ok = false;
   cudaStream_t stream = nullptr;
+  int sms = 0;  // SMs of the device: the persistent product's grid
+  // the driver's tensor-map encoder (through the runtime's entry-point query,
+  // so that the library needs no link against the driver library); null: the
+  // persistent TMA product is unavailable and every product takes the
+  // per-tile kernel
+  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
 };
 
 MlpCtx& mctx() {
@@ -482,9 +759,34 @@ MlpCtx& mctx() {
     if (cudaFuncSetAttribute(fpe::mlp::k_gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              fpe::mlp::kSmemBytes) != cudaSuccess)
       return;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess && fn &&
+        cudaFuncSetAttribute(fpe::mlp::k_gemm_bf16_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             fpe::mlp::kPSmemBytes) == cudaSuccess)
+      c.encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     c.ok = true;
   });
   return c;
+}
+
+// Tensor map of a K-contiguous BF16 matrix (rows x K, row stride ld
+// elements): boxes of 64 K-elements (128 bytes) x box_rows rows in the
+// 128-byte swizzled layout; rows past the end read as zeros.
+int make_map(CUtensorMap* m, const bf16* base, int rows, int K, int ld, int box_rows) {
+  const cuuint64_t dims[2] = {cuuint64_t(K), cuuint64_t(rows)};
+  const cuuint64_t strides[1] = {cuuint64_t(ld) * sizeof(bf16)};
+  const cuuint32_t box[2] = {cuuint32_t(fpe::mlp::kChunkK), cuuint32_t(box_rows)};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = mctx().encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dims, strides,
+                                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -1;
 }
 
 int launch_gemm(const fpe::mlp::GemmParams& P, cudaStream_t s) {
@@ -496,6 +798,18 @@ int launch_gemm(const fpe::mlp::GemmParams& P, cudaStream_t s) {
   if (P.Cb && (P.ldcb % 8 || (reinterpret_cast<uintptr_t>(P.Cb) & 15))) return -1;
   if (P.tn < 16 || P.tn > kTileN || P.tn % 16 || P.ksplit < 1) return -1;
   if (P.ksplit > 1 && !(P.epi == EPI_F32 && P.atomic && !P.bias && !P.act && !P.Cb && !P.CbT)) return -1;
+  if (P.ksplit == 1 && P.K % kChunkK == 0 && mctx().encode) {
+    // persistent product: N-tiles as wide as N allows, one CTA per SM
+    GemmParams Q = P;
+    Q.tn = std::min(P.N, kTileN);
+    CUtensorMap ma, mb;
+    if (make_map(&ma, P.A, P.M, P.K, P.lda, kTileM) == 0 && make_map(&mb, P.B, P.N, P.K, P.ldb, Q.tn) == 0) {
+      const int tiles = (P.M / kTileM) * ((P.N + Q.tn - 1) / Q.tn);
+      k_gemm_bf16_tma<<<std::min(tiles, mctx().sms), kPThreads, kPSmemBytes, s>>>(ma, mb, Q);
+      MK(cudaGetLastError());
+      return 0;
+    }
+  }
   const dim3 grid(P.M / kTileM, (P.N + P.tn - 1) / P.tn, P.ksplit);
   k_gemm_bf16_tc<<<grid, kThreads, kSmemBytes, s>>>(P);
   MK(cudaGetLastError());

@@ -27,9 +27,13 @@ def _bf16_tensor(torch, a):
     return torch.tensor(a, dtype=torch.float32, device="cuda").to(torch.bfloat16).contiguous()
 
 
+# K a multiple of 64 takes the persistent TMA product (51200 rows: 400 tiles,
+# so CTAs loop over several tiles and both TMEM accumulators), K = 16 the
+# per-tile product.
 @pytest.mark.parametrize("M,N,K,bias,act", [(256, 256, 256, False, 0), (128, 16, 256, False, 0),
                                             (384, 48, 16, True, 1), (128, 512, 64, True, 0),
-                                            (256, 256, 4096, False, 0)])
+                                            (256, 256, 4096, False, 0), (51200, 256, 256, True, 1),
+                                            (640, 144, 128, True, 0)])
 def test_tensor_core_gemm_matches_cpu(engine, M, N, K, bias, act):
     from fpe_option_b200 import _lib
     from oracle.mlp_oracle import bf16, silu
