@@ -254,9 +254,11 @@ def main():
                     help="skip the knock-in workload's compact summary in the batch line")
     ap.add_argument("--plain-sample", type=int, default=8,
                     help="contracts timed on the plain one-solve-per-launch FP64 path")
-    ap.add_argument("--workload", default="batch", choices=["batch", "barrier", "surrogate", "calibration"],
+    ap.add_argument("--workload", default="batch",
+                    choices=["batch", "barrier", "surrogate", "calibration", "layer"],
                     help="batch: the batched FPE pricing line (default); surrogate / calibration: "
-                         "the learned part's measurements")
+                         "the learned part's measurements; layer: the surrogate network's forward alone "
+                         "(65,536 rows, random weights), the case its product kernel is profiled on")
     ap.add_argument("--train", type=int, default=65536, help="surrogate training prices")
     ap.add_argument("--surfaces", type=int, default=5, help="calibration: seeded surfaces")
     ap.add_argument("--surrogate-file", default=None,
@@ -271,6 +273,8 @@ def main():
         return run_reference_arm(args)
     if args.workload == "barrier":
         return run_barrier_workload(args)
+    if args.workload == "layer":
+        return run_layer_workload(args)
     if args.workload != "batch":
         return run_learned_workload(args)
 
@@ -570,6 +574,42 @@ def _train_surrogate(args, kind, n_train, log, epochs, batch):
                 "final_losses": losses, "held_out": held}
 
 
+def run_layer_workload(args):
+    """The surrogate network's forward (12 -> 256 x 4 -> 1, random weights) on
+    65,536 random rows: per forward, one input-layer product (K = 16), three
+    65,536 x 256 x 256 layer products (the persistent TMA kernel) and the output
+    layer.  Warm-up forwards first, then `steps` timed ones (CUDA events)."""
+    import torch
+
+    from fpe_option_b200 import build
+    from fpe_option_b200.surrogate import Mlp
+
+    build.build_library()
+    n = 65536
+    net = Mlp(n_in=12, hidden=256, layers=4, max_rows=n, seed=1 + args.seed)
+    x = torch.randn(n, 12, device="cuda", generator=torch.Generator("cuda").manual_seed(args.seed))
+    y = torch.empty(n, device="cuda")
+    for _ in range(max(args.warmup, 3)):
+        net.forward_dev(x, y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        net.forward_dev(x, y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    flops = 2.0 * n * (16 * 256 + 3 * 256 * 256 + 256)
+    print(json.dumps({"metric": "surrogate network forward, 65536 rows", "value": n / (ms / 1000.0),
+                      "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+                      "ms_per_step": ms, "higher_is_better": True, "dtype": "bf16/f32", "data": "synthetic",
+                      "workload": "layer", "tflops": flops / (ms / 1000.0) / 1e12,
+                      "config": {"workload": "MLP 12-256x4-1 SiLU, random weights, 65536 random rows"}}),
+          flush=True)
+    net.close()
+    return 0
+
+
 def run_learned_workload(args):
     import torch
 
@@ -628,7 +668,7 @@ def run_learned_workload(args):
     surfaces = []
     kw = {"grid": SUR_GRID}
     noise = 1e-4 * 100.0
-    res = {"fpe_only": [], "surrogate": [], "hybrid": []}
+    res = {"fpe_only": [], "surrogate": [], "defect": [], "hybrid": []}
     for k in range(args.surfaces):
         rng = np.random.default_rng(4242 + 97 * k + args.seed)
         truth = np.array([rng.uniform(0.8, 2.5), rng.uniform(0.03, 0.12), rng.uniform(0.2, 0.7),
@@ -643,8 +683,10 @@ def run_learned_workload(args):
         x_f, i_f = calibrate_fpe(surf, x0, **kw)
         x_s, i_s = calibrate_with_surrogate(surf, pr, x0, max_iter=50, polish="none", quote_noise=noise,
                                             polish_iter=30, fpe_kw=kw)
+        x_d, i_d = calibrate_with_surrogate(surf, pr, x0, max_iter=50, polish="defect", fpe_kw=kw)
         x_h, i_h = calibrate_with_surrogate(surf, pr, x0, max_iter=50, polish="hybrid", polish_iter=30, fpe_kw=kw)
-        for name, x, inf in (("fpe_only", x_f, i_f), ("surrogate", x_s, i_s), ("hybrid", x_h, i_h)):
+        for name, x, inf in (("fpe_only", x_f, i_f), ("surrogate", x_s, i_s), ("defect", x_d, i_d),
+                             ("hybrid", x_h, i_h)):
             inf = dict(inf)
             inf["max_rel_param_err"] = float(np.max(np.abs(x - truth) / np.abs(truth)))
             inf["x"] = x.tolist()
@@ -657,15 +699,18 @@ def run_learned_workload(args):
                       "mean_max_rel_param_err": float(np.mean([d["max_rel_param_err"] for d in lst])),
                       "median_max_rel_param_err": float(np.median([d["max_rel_param_err"] for d in lst]))}
     line = {"metric": "Heston calibration wall time: surrogate-in-loop vs FPE-only (same GPU)",
-            "value": summ["fpe_only"]["seconds_total"] / summ["surrogate"]["seconds_total"],
+            "value": summ["fpe_only"]["seconds_total"] / summ["defect"]["seconds_total"],
             "unit": "x speed-up", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
             "workload": "calibration",
             "config": {"workload": f"{args.surfaces} seeded surfaces of 15 strikes (K/S0 0.7-1.3) x 8 maturities "
                                    "(0.1-2.0), European calls, FP64 FPE prices + N(0, 1e-4 S0) noise, "
                                    f"{SUR_GRID[0]}x{SUR_GRID[1]} grids; surrogate: LM on the ensemble, one FPE "
                                    "verification, FPE polish only if the FPE residual RMS exceeds 1.5x the noise; "
-                                   "hybrid: FPE residuals with surrogate Jacobians"},
-            "summary": summ, "hybrid_speedup": summ["fpe_only"]["seconds_total"] / summ["hybrid"]["seconds_total"],
+                                   "defect (the headline): LM on the surrogate corrected by its defect against one FPE "
+                                   "pricing of the surface per outer iteration, up to 3; hybrid: FPE residuals with "
+                                   "surrogate Jacobians"},
+            "summary": summ, "surrogate_only_speedup": summ["fpe_only"]["seconds_total"] / summ["surrogate"]["seconds_total"],
+            "hybrid_speedup": summ["fpe_only"]["seconds_total"] / summ["hybrid"]["seconds_total"],
             "truths": surfaces, "runs": res, "surrogate_training": info}
     print(json.dumps(line), flush=True)
     pr.close()

@@ -37,6 +37,16 @@ FPE residual (the surrogate's Jacobian is no descent direction there, e.g.
 at a fit pinned to the edge of its training box), FPE Jacobians finish the
 polish.  ``polish="fpe"`` uses FPE Jacobians throughout; ``polish="none"`` keeps the surrogate's fit if its FPE
 residual RMS is within ``noise_ratio`` times the quotes' noise level.
+
+``polish="defect"`` corrects the surrogate instead of polishing on the FPE
+solver (defect correction, also known as output space mapping): at the
+current fit x_k one FPE pricing of the surface gives the surrogate's defect
+d_k = p_FPE(x_k) - p_sur(x_k), and LM on the corrected surrogate
+p_sur(x) + d_k - quotes gives x_{k+1}.  A fixed point satisfies
+J_sur^T (p_FPE(x) - quotes) = 0, the hybrid polish's condition, while each
+outer iteration costs one FPE pricing of the surface and a surrogate fit of
+microsecond residuals; the defect varies slowly in x, so two or three
+iterations settle it.
 """
 from __future__ import annotations
 
@@ -315,6 +325,21 @@ class HybridSurface:
         return self.fpe.residual(x), J
 
 
+class DefectSurface:
+    """The surrogate's residual plus a fixed defect vector (FPE minus surrogate
+    prices at the last outer iterate)."""
+
+    def __init__(self, sur: SurrogateSurface, defect: np.ndarray):
+        self.sur, self.defect = sur, defect
+
+    def residual(self, x):
+        return self.sur.residual(x) + self.defect
+
+    def jacobian(self, x):
+        r, J = self.sur.jacobian(x)
+        return r + self.defect, J
+
+
 def calibrate_reference_objective(surface: Surface, x0, max_iter=50, tol=1e-8, **kw):
     """The reference Calibrator (calibrator.mojo:87-119): LM with lambda 1e-3,
     x10 / x0.1 (lm.mojo:29-121) on the reference objective, the parameters
@@ -337,8 +362,10 @@ def calibrate_fpe(surface: Surface, x0, max_iter=40, tol=1e-10, **kw):
 
 def calibrate_with_surrogate(surface: Surface, pricer, x0, max_iter=50, tol=1e-10,
                              polish: str = "hybrid", quote_noise: float | None = None,
-                             noise_ratio: float = 1.5, polish_iter: int = 10, fpe_kw=None):
-    """Surrogate-in-loop LM, FPE verification, optional FPE polish."""
+                             noise_ratio: float = 1.5, polish_iter: int = 10, fpe_kw=None,
+                             defect_iter: int = 3, defect_xtol: float = 1e-4):
+    """Surrogate-in-loop LM, FPE verification, optional FPE polish or defect
+    correction (see the module notes)."""
     fpe_kw = fpe_kw or {}
     t = time.perf_counter()
     sb = SurrogateSurface(surface, pricer, grid=fpe_kw.get("grid", (48, 24)))
@@ -354,7 +381,23 @@ def calibrate_with_surrogate(surface: Surface, pricer, x0, max_iter=50, tol=1e-1
     polished = False
     it_polish = 0
     polish_used = polish
-    if polish == "hybrid":
+    if polish == "defect":
+        # r_fpe = p_FPE(x) - quotes, r_sur = p_sur(x) - quotes: their difference is the defect
+        for _ in range(defect_iter):
+            d = r_fpe - r_sur
+            db = DefectSurface(sb, d)
+            cor = levenberg_marquardt(db.residual, db.jacobian, x, max_iter=max_iter, tol=tol, xtol=1e-5,
+                                      ftol=1e-6, max_rejects=6)
+            x_new = clamp(SurrogateSurface.project(cor.x))
+            it_polish += 1
+            step = float(np.max(np.abs(x_new - x) / np.maximum(np.abs(x), 1e-8)))
+            x = x_new
+            r_fpe = fb.residual(x)
+            r_sur = sb.residual(x)
+            if step < defect_xtol:
+                break
+        polished = True
+    elif polish == "hybrid":
         hb = HybridSurface(fb, sb)
         # near-Gauss-Newton steps: the fit starts close to the optimum
         pol = levenberg_marquardt(hb.residual, hb.jacobian, x, max_iter=polish_iter, tol=tol,

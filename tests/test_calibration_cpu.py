@@ -136,3 +136,57 @@ def test_interpolate_pdf_rejects_bad_shapes_before_any_device_work():
         fpe.interpolate_pdf([0.0], [0.0, 1.0], np.zeros((1, 2)), [0.5], [0.5])
     with pytest.raises(ValueError):
         fpe.interpolate_pdf([0.0, 1.0], [0.0, 1.0], np.zeros((2, 2)), [0.5, 0.7], [0.5])
+
+
+def test_defect_correction_reaches_the_fpe_fit(monkeypatch):
+    """A surrogate that is off by a 5 % perturbation of the FPE model's linear
+    map plus a bias fits the quotes to a wrong x on its own; defect correction
+    (each outer iteration: one FPE pricing at the fit, then LM on the surrogate
+    plus that defect) contracts the error by about the perturbation's size per
+    iteration, so three iterations reach the FPE fit to ~1e-4 of the start."""
+    from fpe_option_b200 import calibration as cal
+
+    rng = np.random.default_rng(7)
+    A = rng.standard_normal((15, 5))
+    As = A * (1.0 + 0.05 * rng.standard_normal(A.shape))
+    bias = 0.05 * rng.standard_normal(15)
+
+    class FakeFpe(cal._Backend):
+        def __init__(self, surface, **kw):
+            super().__init__(surface)
+
+        def steps(self, x):
+            return 1e-6 * (1.0 + np.abs(x))
+
+        def price_sets(self, xs):
+            self.contracts_priced += len(xs) * len(self.surface.strikes)
+            return np.atleast_2d(xs) @ A.T
+
+    class FakeSur(cal._Backend):
+        @classmethod
+        def project(cls, x):
+            return np.asarray(x, np.float64)
+
+        def __init__(self, surface, pricer, grid=None):
+            super().__init__(surface)
+            self.fallback_quotes = 0
+
+        def steps(self, x):
+            return 1e-6 * (1.0 + np.abs(x))
+
+        def price_sets(self, xs):
+            return np.atleast_2d(xs) @ As.T + bias
+
+    monkeypatch.setattr(cal, "FpeSurface", FakeFpe)
+    monkeypatch.setattr(cal, "SurrogateSurface", FakeSur)
+    surf = cal.Surface.grid(100.0, 0.02, [0.9, 1.0, 1.1], [0.5, 1.0, 1.5, 2.0, 2.5])
+    truth = np.array([1.5, 0.06, 0.4, -0.5, 0.05])
+    surf.prices = truth @ A.T
+    x0 = truth + np.array([-0.4, 0.02, -0.1, 0.2, 0.02])
+    # a noise level above any residual keeps the surrogate's own fit (no FPE polish)
+    x_plain, _ = cal.calibrate_with_surrogate(surf, _Pricer(), x0, polish="none", quote_noise=1e6)
+    x_def, info = cal.calibrate_with_surrogate(surf, _Pricer(), x0, polish="defect", defect_iter=3,
+                                               defect_xtol=0.0)
+    err0 = np.abs(x0 - truth).max()
+    assert np.abs(x_plain - truth).max() > 1e-2 * err0  # the surrogate alone misses
+    assert np.abs(x_def - truth).max() < 1e-3 * err0, (x_def, truth, info)
