@@ -76,43 +76,119 @@ __device__ __forceinline__ double* vslot(const RadauCtx& C, int k) { return C.wo
 
 // Y_r = sum_t c_t (S_t (x) V_t) X_r, r < nrhs.  Two passes:
 // T_{t,r} = X_r V_t^T, then Y_r = sum_t c_t S_t T_{t,r}.
-static __device__ void kron_apply(const RadauCtx& C, const KronTerm* terms, int nt, const double* const* X,
-                           double* const* Y, int nrhs) {
-  const int nv = C.nv, ns = C.ns, N = C.N;
-  double* T = (C.tsm && !*C.err && nt * nrhs * N <= C.tsm_cap) ? C.tsm : vslot(C, RV_TMP);
-  for (int e = threadIdx.x; e < nt * nrhs * N; e += blockDim.x) {
-    const int tr = e / N, idx = e - tr * N;
-    const int t = tr / nrhs, r = tr - t * nrhs;
-    const int i = idx / nv, j = idx - i * nv;
-    const double* V = terms[t].V + j * 7;
-    const double* x = X[r] + i * nv;
-    double acc = 0.0;
+//
+// One out-of-line instance per (terms, right-hand sides, intermediate in
+// shared memory): the terms and vectors arrive by value and are indexed with
+// compile-time indices only, so none of them is read from the kernel's stack
+// frame inside the loops (such slots must be reloaded after every store
+// through a global pointer); the factors and a shared intermediate are read
+// through shared-space pointers.  A thread takes one grid point per pass and
+// all terms and right-hand sides of it, so X's band is loaded once for every
+// term.  Each output is the same sum, in the same order, as one term and one
+// right-hand side at a time.
+struct KronArgs {
+  int ns, nv, N;
+  double* T;  // the intermediate: NT x NR vectors of N
+  const double *S[5], *V[5];
+  double c[5];
+  const double* X[3];
+  double* Y[3];
+};
+
+template <int NT, int NR, bool TSH>
+static __device__ __noinline__ void kron_apply_t(KronArgs a) {
+  const int nv = a.nv, ns = a.ns, N = a.N;
+  auto sh = [](const double* p) { return reinterpret_cast<const double*>(fpe_dsmem + dsmem_offset(p)); };
+  const double* S[NT];
+  const double* V[NT];
 #pragma unroll
-    for (int dd = 0; dd < 7; ++dd) {
-      const int l = j + dd - 3;
-      if (l >= 0 && l < nv) acc += V[dd] * x[l];
-    }
-    T[size_t(tr) * N + idx] = acc;
+  for (int t = 0; t < NT; ++t) {
+    S[t] = sh(a.S[t]);
+    V[t] = sh(a.V[t]);
   }
-  __syncthreads();
-  for (int e = threadIdx.x; e < nrhs * N; e += blockDim.x) {
-    const int r = e / N, idx = e - r * N;
+  double* T = TSH ? reinterpret_cast<double*>(fpe_dsmem + dsmem_offset(a.T)) : a.T;
+  for (int idx = threadIdx.x; idx < N; idx += blockDim.x) {
     const int i = idx / nv, j = idx - i * nv;
-    double acc = 0.0;
-    for (int t = 0; t < nt; ++t) {
-      const double* S = terms[t].S + i * 7;
-      const double* Tt = T + size_t(t * nrhs + r) * N;
-      double a = 0.0;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      const double* x = a.X[r] + i * nv;
+      double xs[7];
 #pragma unroll
       for (int dd = 0; dd < 7; ++dd) {
-        const int k = i + dd - 3;
-        if (k >= 0 && k < ns) a += S[dd] * Tt[k * nv + j];
+        const int l = j + dd - 3;
+        xs[dd] = (l >= 0 && l < nv) ? x[l] : 0.0;
       }
-      acc += terms[t].c * a;
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const double* Vt = V[t] + j * 7;
+        double acc = 0.0;
+#pragma unroll
+        for (int dd = 0; dd < 7; ++dd) {
+          const int l = j + dd - 3;
+          if (l >= 0 && l < nv) acc += Vt[dd] * xs[dd];
+        }
+        T[size_t(t * NR + r) * N + idx] = acc;
+      }
     }
-    Y[r][idx] = acc;
   }
   __syncthreads();
+  for (int idx = threadIdx.x; idx < N; idx += blockDim.x) {
+    const int i = idx / nv, j = idx - i * nv;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      double acc = 0.0;
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const double* St = S[t] + i * 7;
+        const double* Tt = T + size_t(t * NR + r) * N;
+        double s = 0.0;
+#pragma unroll
+        for (int dd = 0; dd < 7; ++dd) {
+          const int k = i + dd - 3;
+          if (k >= 0 && k < ns) s += St[dd] * Tt[k * nv + j];
+        }
+        acc += a.c[t] * s;
+      }
+      a.Y[r][idx] = acc;
+    }
+  }
+  __syncthreads();
+}
+
+template <int NT, int NR>
+static __device__ __forceinline__ void kron_apply_n(const KronArgs& a, bool tsh) {
+  if (tsh) kron_apply_t<NT, NR, true>(a);
+  else kron_apply_t<NT, NR, false>(a);
+}
+
+static __device__ void kron_apply(const RadauCtx& C, const KronTerm* terms, int nt, const double* const* X,
+                                  double* const* Y, int nrhs) {
+  const int N = C.N;
+  const bool tsh = C.tsm && !*C.err && nt * nrhs * N <= C.tsm_cap;
+  KronArgs a;
+  a.ns = C.ns;
+  a.nv = C.nv;
+  a.N = N;
+  a.T = tsh ? C.tsm : vslot(C, RV_TMP);
+  for (int t = 0; t < 5; ++t) {
+    a.S[t] = t < nt ? terms[t].S : nullptr;
+    a.V[t] = t < nt ? terms[t].V : nullptr;
+    a.c[t] = t < nt ? terms[t].c : 0.0;
+  }
+  for (int r = 0; r < 3; ++r) {
+    a.X[r] = r < nrhs ? X[r] : nullptr;
+    a.Y[r] = r < nrhs ? Y[r] : nullptr;
+  }
+  // the (terms, right-hand sides) pairs the solver uses
+  if (nt == 4 && nrhs == 1) kron_apply_n<4, 1>(a, tsh);
+  else if (nt == 4 && nrhs == 3) kron_apply_n<4, 3>(a, tsh);
+  else if (nt == 5 && nrhs == 1) kron_apply_n<5, 1>(a, tsh);
+  else if (nt == 5 && nrhs == 2) kron_apply_n<5, 2>(a, tsh);
+  else if (nt == 1 && nrhs == 1) kron_apply_n<1, 1>(a, tsh);
+  else if (nt == 1 && nrhs == 2) kron_apply_n<1, 2>(a, tsh);
+  else if (nt == 1 && nrhs == 3) kron_apply_n<1, 3>(a, tsh);
+  else if (nt == 4 && nrhs == 2) kron_apply_n<4, 2>(a, tsh);
+  else if (nt == 5 && nrhs == 3) kron_apply_n<5, 3>(a, tsh);
 }
 
 struct RadauSmem {
