@@ -347,18 +347,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16_tc(GemmParams P) {
 //   warp 1 (one lane): tcgen05.mma of each chunk into one of two TMEM
 //     accumulators, tcgen05.commit to the stage's "empty" barrier, and after a
 //     tile's last chunk to the accumulator's "full" barrier;
-//   warps 2..17: the epilogue of a finished accumulator (warp w reads TMEM
-//     lanes 32 (w % 4) .. + 31, the four warps of a lane quarter take turns
-//     at 16-column chunks), then an arrival on its "empty" barrier;
+//   warps 2..9: the epilogue of a finished accumulator (warp w reads TMEM
+//     lanes 32 (w % 4) .. + 31, the two warps of a lane quarter split the
+//     columns; BF16 outputs leave through a per-warp shared staging tile as
+//     whole 128-byte row segments), then an arrival on its "empty" barrier;
 // so the loads of later chunks, the MMAs of tile i + 1 and the epilogue of
 // tile i overlap.  Every wait is bounded: a wait that gives up sets *P.err and
 // ends the CTA's loop, and the copies and MMAs already issued are waited out
 // before the TMEM is released.  The tensor maps describe this GPU's own
 // operands only, and no load is multicast.
-constexpr int kPStages = 4;
-constexpr int kPThreads = 576;  // TMA warp, MMA warp, sixteen epilogue warps
-constexpr int kPStageA = kTileM * 128;  // 128 rows x 64 BF16
-constexpr int kPSmemBytes = kPStages * (kPStageA + kTileN * 128) + 1024;  // + alignment of the swizzle atoms
+constexpr int kPStages = 3;
+constexpr int kPEpiWarps = 8;                    // two per TMEM lane quarter
+constexpr int kPThreads = 64 + 32 * kPEpiWarps;  // TMA warp, MMA warp, epilogue warps
+constexpr int kPStageA = kTileM * 128;           // 128 rows x 64 BF16
+// Dynamic shared memory (offsets from the 1024-byte aligned base): a resident
+// B of up to 128 KB then the A stages, or A + B stages; then one 4 KB staging
+// tile (32 rows x 128 bytes) per epilogue warp for the coalesced BF16 stores.
+constexpr int kPBres = 4 * kTileN * 128;  // 128 KB: K <= 256 at N = 256
+constexpr int kPStagingOff =
+    (kPBres + kPStages * kPStageA) > kPStages * (kPStageA + kTileN * 128) ? kPBres + kPStages * kPStageA
+                                                                           : kPStages * (kPStageA + kTileN * 128);
+constexpr int kPSmemBytes = kPStagingOff + kPEpiWarps * 4096 + 1024;  // + alignment of the swizzle atoms
 
 // Shared-memory matrix descriptor of a K-major operand in the 128-byte
 // swizzled layout that TMA writes (rows of 128 bytes, 8-row groups 1024 bytes
@@ -405,10 +414,10 @@ __global__ void __launch_bounds__(kPThreads, 1)
   // With one N-tile whose B fits the stages' B area (K <= 256 at N = 256), B
   // stays resident: its nk chunks are loaded once, at the start, and the
   // stages carry A alone (a sixth of the bytes per tile at K = N = 256).
-  const bool bres = P.N <= BN && uint32_t(nk) * uint32_t(BN) * 128u <= uint32_t(kPStages * kTileN * 128);
+  const bool bres = P.N <= BN && uint32_t(nk) * uint32_t(BN) * 128u <= uint32_t(kPBres);
   const uint32_t bchunk = uint32_t(BN) * 128u;  // bytes of one B chunk
   const uint32_t stage_bytes = bres ? uint32_t(kPStageA) : uint32_t(kPStageA) + bchunk;
-  const uint32_t abase = bres ? base + uint32_t(kPStages * kTileN * 128) : base;  // stage 0
+  const uint32_t abase = bres ? base + uint32_t(kPBres) : base;  // stage 0
   if (warp == 1) tmem_alloc(&tmem_slot, ncols);
   if (tid == 0) {
     for (int s = 0; s < kPStages; ++s) {
@@ -525,10 +534,15 @@ __global__ void __launch_bounds__(kPThreads, 1)
       mbar_wait_bounded(&done, 0, kBulkWaitLimit);
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, the tile's rows,
-    // and the 16-column chunks h, h + 4, h + 8, ... (h = (w - 2) / 4), two
-    // chunks per completion wait
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, the tile's rows;
+    // the two warps of a lane quarter (h = (w - 2) / 4) split the columns
     const int quarter = warp & 3, row = 32 * quarter + lane, h = (warp - 2) >> 2;
+    // bias + SiLU to BF16 only (the inference layers): 64-column spans 64 h,
+    // 64 h + 128, ... go through this warp's 4 KB staging tile, rows written
+    // with their 16-byte chunks rotated by row (conflict-free), then read back
+    // so that each store instruction writes four whole 128-byte row segments
+    const bool staged = P.epi == EPI_BIAS_SILU && P.Cb && !P.Cf && !P.CbT;
+    unsigned char* const stile = psmem + (base - smem_u32(psmem)) + kPStagingOff + (warp - 2) * 4096;
     int acc = 0;
     uint32_t aph = 0;
     // the warp's decisions are uniform: tcgen05.ld is warp-collective
@@ -541,22 +555,63 @@ __global__ void __launch_bounds__(kPThreads, 1)
       }
       tc_fence_after();
       const uint32_t trow = tmem + (uint32_t(32 * quarter) << 16) + uint32_t(acc) * acc_cols;
-      for (int c = 16 * h; c < Nt; c += 128) {
-        uint32_t r0[16], r1[16];
-        const bool two = c + 64 < Nt;  // uniform in the warp
-        tmem_ld16_async(trow + uint32_t(c), r0);
-        if (two) tmem_ld16_async(trow + uint32_t(c + 64), r1);
-        tmem_wait_ld();
-        float v[16], b[16];
+      if (staged && (Nt & 63) == 0) {
+        for (int c = 64 * h; c < Nt; c += 128) {
+          uint32_t r[4][16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r0[j]);
-        bias16(n0 + c, b);
-        epilogue16(P, b, m0 + row, n0 + c, v);
-        if (two) {
+          for (int k = 0; k < 4; ++k) tmem_ld16_async(trow + uint32_t(c + 16 * k), r[k]);
+          tmem_wait_ld();
 #pragma unroll
-          for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r1[j]);
-          bias16(n0 + c + 64, b);
-          epilogue16(P, b, m0 + row, n0 + c + 64, v);
+          for (int k = 0; k < 4; ++k) {
+            float b[16];
+            bias16(n0 + c + 16 * k, b);
+            uint32_t pk[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              float x0 = __uint_as_float(r[k][2 * j]) + b[2 * j];
+              float x1 = __uint_as_float(r[k][2 * j + 1]) + b[2 * j + 1];
+              x0 *= sigmoidf_(x0);
+              x1 *= sigmoidf_(x1);
+              const __nv_bfloat162 h2 = __floats2bfloat162_rn(x0, x1);
+              pk[j] = *reinterpret_cast<const uint32_t*>(&h2);
+            }
+            // chunks 2k and 2k + 1 of this lane's row
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              const int ch = 2 * k + u;
+              *reinterpret_cast<uint4*>(stile + lane * 128 + ((ch ^ (lane & 7)) << 4)) =
+                  make_uint4(pk[4 * u], pk[4 * u + 1], pk[4 * u + 2], pk[4 * u + 3]);
+            }
+          }
+          __syncwarp();
+#pragma unroll
+          for (int it = 0; it < 8; ++it) {
+            const int rr = 4 * it + (lane >> 3), ch = lane & 7;
+            const uint4 v = *reinterpret_cast<const uint4*>(stile + rr * 128 + ((ch ^ (rr & 7)) << 4));
+            *reinterpret_cast<uint4*>(P.Cb + size_t(m0 + 32 * quarter + rr) * P.ldcb + n0 + c + 8 * ch) = v;
+          }
+          __syncwarp();  // the tile is rewritten by the next span
+        }
+      } else {
+        // 16-column chunks 16 h, 16 h + 64, ... and the chunk 32 columns on
+        // from each, two per completion wait
+        for (int c = 16 * h; c < Nt; c += 64) {
+          uint32_t r0[16], r1[16];
+          const bool two = c + 32 < Nt;  // uniform in the warp
+          tmem_ld16_async(trow + uint32_t(c), r0);
+          if (two) tmem_ld16_async(trow + uint32_t(c + 32), r1);
+          tmem_wait_ld();
+          float v[16], b[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r0[j]);
+          bias16(n0 + c, b);
+          epilogue16(P, b, m0 + row, n0 + c, v);
+          if (two) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r1[j]);
+            bias16(n0 + c + 32, b);
+            epilogue16(P, b, m0 + row, n0 + c + 32, v);
+          }
         }
       }
       tc_fence_before();
