@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t base = (smem_u32(psmem) + 1023u) & ~1023u;  // swizzle atoms are 1024-byte aligned
   const int BN = P.tn;
-  const int tiles_m = P.M / kTileM, ntiles = tiles_m * ((P.N + BN - 1) / BN);
+  const int tiles_m = P.M / kTileM, tiles_n = (P.N + BN - 1) / BN, ntiles = tiles_m * tiles_n;
   const int nk = P.K / kChunkK;
   uint32_t acc_cols = 32;
   while (int(acc_cols) < BN) acc_cols <<= 1;
@@ -414,8 +414,12 @@ __global__ void __launch_bounds__(kPThreads, 1)
   // With one N-tile whose B fits the stages' B area (K <= 256 at N = 256), B
   // stays resident: its nk chunks are loaded once, at the start, and the
   // stages carry A alone (a sixth of the bytes per tile at K = N = 256).
-  const bool bres = P.N <= BN && uint32_t(nk) * uint32_t(BN) * 128u <= uint32_t(kPBres);
-  const uint32_t bchunk = uint32_t(BN) * 128u;  // bytes of one B chunk
+  // When every N-tile's B fits the resident area (N x K <= 256 x 256), all of B
+  // stays in shared memory: chunk kc of the nb = tiles_n x BN rows at
+  // base + kc nb 128, loaded once at the start, and the stages carry A alone.
+  const uint32_t bchunk = uint32_t(BN) * 128u;                    // bytes of one B chunk of one N-tile
+  const uint32_t brow = uint32_t(tiles_n) * bchunk;               // bytes of one B chunk of all N-tiles
+  const bool bres = uint32_t(nk) * brow <= uint32_t(kPBres);
   const uint32_t stage_bytes = bres ? uint32_t(kPStageA) : uint32_t(kPStageA) + bchunk;
   const uint32_t abase = bres ? base + uint32_t(kPBres) : base;  // stage 0
   if (warp == 1) tmem_alloc(&tmem_slot, ncols);
@@ -460,12 +464,14 @@ __global__ void __launch_bounds__(kPThreads, 1)
       uint32_t ph = 0, pend = 0, pend_ph = 0;  // stages with a load in flight, and its phase parity
       const bool any = int(blockIdx.x) < ntiles;
       if (bres && any) {
-        mbar_arrive_expect_tx(&bfull, uint32_t(nk) * bchunk);
+        mbar_arrive_expect_tx(&bfull, uint32_t(nk) * brow);
         for (int kc = 0; kc < nk; ++kc)
-          tma_load_2d(base + uint32_t(kc) * bchunk, &mapB, kc * kChunkK, 0, smem_u32(&bfull));
+          for (int nt = 0; nt < tiles_n; ++nt)
+            tma_load_2d(base + uint32_t(kc) * brow + uint32_t(nt) * bchunk, &mapB, kc * kChunkK, nt * BN,
+                        smem_u32(&bfull));
       }
       for (int t = blockIdx.x; t < ntiles && !give_up; t += gridDim.x) {
-        const int m0 = (t % tiles_m) * kTileM, n0 = (t / tiles_m) * BN;
+        const int m0 = (t / tiles_n) * kTileM, n0 = (t % tiles_n) * BN;
         for (int kc = 0; kc < nk; ++kc) {
           // a fresh barrier counts as having completed the phase before its first
           if (!mbar_wait_bounded(&empty[stage], ph ^ 1u, kBulkWaitLimit)) {
@@ -510,7 +516,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
           }
           tc_fence_after();
           const uint32_t sa = abase + uint32_t(stage) * stage_bytes;
-          const uint32_t sb = bres ? base + uint32_t(kc) * bchunk : sa + kPStageA;
+          const uint32_t sb = bres ? base + uint32_t(kc) * brow + uint32_t(t % tiles_n) * bchunk : sa + kPStageA;
 #pragma unroll
           for (int s = 0; s < kChunkK / 16; ++s)
             umma_bf16(d, umma_desc_sw128(sa + 32u * s), umma_desc_sw128(sb + 32u * s), idesc,
@@ -547,7 +553,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
     uint32_t aph = 0;
     // the warp's decisions are uniform: tcgen05.ld is warp-collective
     for (int t = blockIdx.x; t < ntiles && !__any_sync(0xffffffffu, give_up != 0); t += gridDim.x) {
-      const int m0 = (t % tiles_m) * kTileM, n0 = (t / tiles_m) * BN;
+      const int m0 = (t / tiles_n) * kTileM, n0 = (t % tiles_n) * BN;
       const int Nt = min(BN, P.N - n0);
       if (!__all_sync(0xffffffffu, mbar_wait_bounded(&accf[acc], aph, kBulkWaitLimit))) {
         fail();
@@ -854,7 +860,8 @@ int launch_gemm(const fpe::mlp::GemmParams& P, cudaStream_t s) {
   if (P.tn < 16 || P.tn > kTileN || P.tn % 16 || P.ksplit < 1) return -1;
   if (P.ksplit > 1 && !(P.epi == EPI_F32 && P.atomic && !P.bias && !P.act && !P.Cb && !P.CbT)) return -1;
   if (P.ksplit == 1 && P.K % kChunkK == 0 && mctx().encode) {
-    // persistent product: N-tiles as wide as N allows, one CTA per SM
+    // persistent product, one CTA per SM, N-tiles as wide as N allows (128-wide
+    // tiles at N = 256, for a shorter last wave, measured no faster)
     GemmParams Q = P;
     Q.tn = std::min(P.N, kTileN);
     CUtensorMap ma, mb;
