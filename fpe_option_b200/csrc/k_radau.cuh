@@ -155,6 +155,40 @@ static __device__ __noinline__ void kron_apply_t(KronArgs a) {
   __syncthreads();
 }
 
+// Any (nt <= 5, nrhs <= 3): the same sums with run-time loops.
+static __device__ __noinline__ void kron_apply_rolled(KronArgs a, int nt, int nr) {
+  const int nv = a.nv, ns = a.ns, N = a.N;
+  for (int idx = threadIdx.x; idx < N; idx += blockDim.x) {
+    const int i = idx / nv, j = idx - i * nv;
+    for (int r = 0; r < nr; ++r)
+      for (int t = 0; t < nt; ++t) {
+        double acc = 0.0;
+        for (int dd = 0; dd < 7; ++dd) {
+          const int l = j + dd - 3;
+          if (l >= 0 && l < nv) acc += a.V[t][j * 7 + dd] * a.X[r][i * nv + l];
+        }
+        a.T[size_t(t * nr + r) * N + idx] = acc;
+      }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < N; idx += blockDim.x) {
+    const int i = idx / nv, j = idx - i * nv;
+    for (int r = 0; r < nr; ++r) {
+      double acc = 0.0;
+      for (int t = 0; t < nt; ++t) {
+        double s = 0.0;
+        for (int dd = 0; dd < 7; ++dd) {
+          const int k = i + dd - 3;
+          if (k >= 0 && k < ns) s += a.S[t][i * 7 + dd] * a.T[size_t(t * nr + r) * N + k * nv + j];
+        }
+        acc += a.c[t] * s;
+      }
+      a.Y[r][idx] = acc;
+    }
+  }
+  __syncthreads();
+}
+
 template <int NT, int NR>
 static __device__ __forceinline__ void kron_apply_n(const KronArgs& a, bool tsh) {
   if (tsh) kron_apply_t<NT, NR, true>(a);
@@ -179,7 +213,8 @@ static __device__ void kron_apply(const RadauCtx& C, const KronTerm* terms, int 
     a.X[r] = r < nrhs ? X[r] : nullptr;
     a.Y[r] = r < nrhs ? Y[r] : nullptr;
   }
-  // the (terms, right-hand sides) pairs the solver uses
+  // the (terms, right-hand sides) pairs the solver uses; any other pair takes
+  // the rolled instance
   if (nt == 4 && nrhs == 1) kron_apply_n<4, 1>(a, tsh);
   else if (nt == 4 && nrhs == 3) kron_apply_n<4, 3>(a, tsh);
   else if (nt == 5 && nrhs == 1) kron_apply_n<5, 1>(a, tsh);
@@ -187,8 +222,7 @@ static __device__ void kron_apply(const RadauCtx& C, const KronTerm* terms, int 
   else if (nt == 1 && nrhs == 1) kron_apply_n<1, 1>(a, tsh);
   else if (nt == 1 && nrhs == 2) kron_apply_n<1, 2>(a, tsh);
   else if (nt == 1 && nrhs == 3) kron_apply_n<1, 3>(a, tsh);
-  else if (nt == 4 && nrhs == 2) kron_apply_n<4, 2>(a, tsh);
-  else if (nt == 5 && nrhs == 3) kron_apply_n<5, 3>(a, tsh);
+  else kron_apply_rolled(a, nt, nrhs);
 }
 
 struct RadauSmem {
