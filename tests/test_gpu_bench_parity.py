@@ -95,3 +95,29 @@ def test_knock_in_workload_vs_oracle(engine, oracle):
     assert (s64 == 0).all() and (s32 == 0).all()
     assert _rel(p64, ref).max() < 1e-5, _rel(p64, ref)
     assert _rel(p32, ref).max() < 1e-4, _rel(p32, ref)
+
+
+@pytest.mark.parametrize("block_split", [1, 2])
+def test_hard_stage_matrices_vs_oracle(engine, oracle, block_split):
+    """The block LU pivots only inside each pivot block (Gauss-Jordan with
+    partial pivoting), never across block rows.  The least diagonally dominant
+    stage matrices come from low-Feller parameters (2 kappa theta / sigma^2
+    well below 1: strong v-diffusion against weak mean reversion), long
+    maturities (the largest steps, up to the T/5 cap) and the exact Radau
+    constants, factored in FP32.  On such contracts, on the largest config
+    grids, the FP32 and FP64 factor paths still match the oracle (which solves
+    with pivoted sparse LU) to the workload tolerances."""
+    fpe = engine
+    rows = []
+    for kappa, theta, sigma, rho, T, K in ((0.3, 0.02, 0.9, -0.9, 2.0, 100.0), (0.5, 0.03, 1.0, -0.7, 2.0, 120.0),
+                                          (0.2, 0.04, 0.8, 0.0, 1.5, 90.0), (0.4, 0.02, 1.2, -0.5, 2.0, 80.0)):
+        assert 2 * kappa * theta / sigma ** 2 < 0.1
+        rows.append([kappa, theta, sigma, rho, 0.04, T, 100.0, 0.03, K, 0.0, 0.0, 300.0])
+    P = np.array(rows)
+    I = np.array([[64, 32, 8], [64, 32, 9], [48, 24, 8], [64, 24, 9]], np.int32)
+    ref = _oracle(oracle, P, I)
+    p64, s64 = fpe.price_batch(P, I, _opts(fpe, 0, block_split=block_split))
+    p32, s32 = fpe.price_batch(P, I, _opts(fpe, 1, block_split=block_split))
+    assert (s64 == 0).all() and (s32 == 0).all(), (s64, s32)
+    assert _rel(p64, ref).max() < 1e-6, _rel(p64, ref)
+    assert _rel(p32, ref).max() < 1e-4, _rel(p32, ref)
