@@ -61,3 +61,19 @@ def test_class_batch_is_seeded_and_of_one_class(tuner):
     P2, _ = tuner.class_batch(48, 24, 6, seed=3)
     assert np.array_equal(P, P2)
     assert (I[:, 0] == 48).all() and (I[:, 1] == 24).all() and set(I[:, 2]) == {8, 9}
+
+
+def test_shipped_table_covers_both_workloads():
+    """The B200 table in the package names every grid class of the batched and
+    knock-in workloads once (config discretization, FP32 factors, direct
+    complex stage), with a valid shape; half-width blocks exactly where nv x nv
+    scratch would not fit shared memory (n_v = 48)."""
+    from fpe_option_b200 import autotune
+
+    rows = autotune.parse(autotune.DEFAULT_TABLE)
+    keys = [(r["n_s"], r["n_v"]) for r in rows]
+    assert sorted(keys) == sorted(set(autotune.BATCH_CLASSES) | set(autotune.BARRIER_CLASSES))
+    for r in rows:
+        assert (r["disc"], r["precision"], r["complex_solve"]) == (1, 1, 2)
+        assert (r["block_split"], r["sweep_buffers"]) in autotune.CANDIDATES
+        assert r["block_split"] == (2 if r["n_v"] == 48 else 1), r
